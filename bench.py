@@ -1,0 +1,345 @@
+#!/usr/bin/env python
+"""Benchmark: FP64 energy+gradient evaluations/s of the NECG objective
+(outprod, python/outprod.py:20-76) on LiH, n=5, K=1024, nst=24.
+
+One step = one full evaluation (H, S, E, gradient of E with respect to all
+K*30 + K parameters) of the seeded synthetic LiH K=1024 basis.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl engine|reference]
+
+* value: whole-job evals/s with x resident on the device, device-timed with
+  CUDA events on the launch stream (sum of per-step times; a 256 MiB buffer is
+  written between steps to flush L2 and is not timed), max over ranks.
+* e2e: the same metric through the C-ABI host-pointer entry point
+  necg_outprod_host: pinned host x in, host f and g out, copies timed.
+* roofline: the gradient-tile kernel (the dominant one): algorithmic FP64
+  FLOPs per launch (counted from the kernel's own templates) / its live
+  CUDA-event duration, against the FP64 FMA throughput measured on this GPU.
+* cpu_baseline: the oracle (a C restatement of the reference's matel/gradel
+  loops) on all host cores over a random sample of the workload's terms,
+  extrapolated to evals/s.
+* --impl reference: the same CPU port timed as the reference arm.
+Multi-GPU (torchrun): every rank evaluates its own replica of the workload
+(no collective on the data path); value = all ranks' evals / max rank time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+METRIC = "FP64 energy+grad evals/s, LiH K=1024 (dE<1e-10 Eh); served p50/p99 latency"
+WORKLOADS = {"lih_k1024": "LiH n=5 K=1024 nst=24 efs=-2e-4, seed 1, C=1/K",
+             "h2_k2048": "H2 n=3 K=2048 nst=4, seed 2, C=1/K",
+             "lih_k12": "LiH n=5 K=12 nst=24, seed 0"}
+PHASES = ["prep", "energy", "finalize", "grad_tiles", "grad_reduce"]
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--workload", default="lih_k1024", choices=sorted(WORKLOADS))
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU-baseline sample budget")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+# ----------------------------------------------------------------------------- CPU port
+def cpu_port_rate(prob, seconds: float, seed: int = 0):
+    """evals/s of the oracle port over a random sample of the workload's terms,
+    using every host core (one ctypes call per chunk; ctypes releases the GIL)."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    from oracle.oracle import Oracle
+    o = Oracle.from_problem(prob)
+    K, nst = prob.K, prob.nst
+    n_mat, n_grad = K * (K + 1) // 2 * nst, K * K * nst  # calls per evaluation
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    rng = np.random.default_rng(seed)
+
+    def terms(count, lower):
+        stf = rng.integers(1, nst + 1, count)
+        i = rng.integers(1, K + 1, count)
+        j = rng.integers(1, K + 1, count)
+        if lower:
+            i, j = np.maximum(i, j), np.minimum(i, j)
+        return np.stack([stf, i, j], 1).astype(np.int32)
+
+    # calibrate on one core
+    cal_m, cal_g = terms(200, True), terms(400, False)
+    t0 = time.perf_counter()
+    o.sample_terms(prob.iv, cal_m, cal_g)
+    per = (time.perf_counter() - t0) / 600.0
+    frac = min(1.0, seconds * cores / (per * (n_mat + n_grad)))
+    nm, ng = max(cores, int(frac * n_mat)), max(cores, int(frac * n_grad))
+    mt, gt = terms(nm, True), terms(ng, False)
+    chunks = [(mt[c::cores], gt[c::cores]) for c in range(cores)]
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(cores) as ex:
+        list(ex.map(lambda c: o.sample_terms(prob.iv, c[0], c[1]), chunks))
+    wall = time.perf_counter() - t0
+    evals = 0.5 * (nm / n_mat + ng / n_grad)
+    return {"value": evals / wall, "unit": "evals/s", "cores": cores, "kind": "port",
+            "sample": f"{nm} matel + {ng} gradel terms ({100 * evals:.3f}% of one evaluation's "
+                      f"{n_mat} + {n_grad}), {wall:.1f} s wall on {cores} threads, extrapolated"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from nbo_correlatedgaussians_b200 import synth
+    prob = synth.workload(args.workload)
+    per_step = max(1.0, 150.0 / max(1, args.steps + args.warmup))
+    per_step = min(per_step, 6.0)
+    for w in range(args.warmup):
+        cpu_port_rate(prob, per_step / 3, seed=100 + w)
+    rates, walls, last = [], [], None
+    for s in range(args.steps):
+        t0 = time.perf_counter()
+        last = cpu_port_rate(prob, per_step, seed=s)
+        walls.append(time.perf_counter() - t0)
+        rates.append(last["value"])
+    value = statistics.mean(rates)
+    out = {"metric": METRIC, "value": value, "unit": "evals/s", "impl": "reference", "n_gpus": args.gpus,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * statistics.mean(walls),
+           "ms_per_eval_extrapolated": 1e3 / value, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded, oldquit.dat layout)",
+           "config": {"workload": args.workload, "desc": WORKLOADS[args.workload]},
+           "cpu_baseline": dict(last, value=value),
+           "e2e": {"value": value, "unit": "evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+           "note": "reference arm = oracle/ C port of the reference's matel/gradel loops (the reference "
+                   "itself is Python and cannot travel to the GPU box); each step times a bounded random "
+                   "sample of the evaluation's terms on all host threads"}
+    print(json.dumps(out), flush=True)
+
+
+# ----------------------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.idx), "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, power, reasons = [], [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+                power.append(float(parts[3]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "power_w_max": max(power),
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+# ----------------------------------------------------------------------------- engine arm
+def run_engine(args):
+    import ctypes
+
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py needs a CUDA device")
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    from nbo_correlatedgaussians_b200 import _lib, synth
+    from nbo_correlatedgaussians_b200.engine import Engine, term_flops
+    L = _lib.lib()
+    prob = synth.workload(args.workload)
+    eng = Engine(prob)
+    _lib.check(L.necg_profile(eng.h, 1), "necg_profile")
+    stream = torch.cuda.current_stream()
+    x = torch.from_numpy(prob.x).cuda()
+    g = torch.empty_like(x)
+    f = torch.empty(1, dtype=torch.float64, device="cuda")
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def step():
+        rc = L.necg_outprod(eng.h, prob.K, x.data_ptr(), f.data_ptr(), g.data_ptr(), None, None,
+                            stream.cuda_stream)
+        _lib.check(rc, "necg_outprod")
+
+    phase_buf = (ctypes.c_double * 5)()
+    for _ in range(args.warmup):
+        flush.fill_(1.0)
+        step()
+    eng.raise_status("warm-up")
+    peak = ctypes.c_double(0.0)
+    _lib.check(L.necg_fp64_peak(200000, ctypes.byref(peak), stream.cuda_stream), "necg_fp64_peak")
+
+    clocks = ClockSampler(local) if rank == 0 else None
+    if clocks:
+        clocks.start()
+    barrier()
+    step_ms, phases = [], []
+    for _ in range(args.steps):
+        flush.fill_(float(len(step_ms)))
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        step()
+        e1.record(stream)
+        _lib.check(L.necg_phase_ms(eng.h, phase_buf), "necg_phase_ms")
+        e1.synchronize()
+        step_ms.append(e0.elapsed_time(e1))
+        phases.append(list(phase_buf))
+    barrier()
+    clk = clocks.stop() if clocks else None
+    eng.raise_status("timed steps")
+    E = float(f.item())
+    total = torch.tensor([sum(step_ms)], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(total, op=dist.ReduceOp.MAX)
+    total_ms = float(total.item())
+    value = world * args.steps / (total_ms * 1e-3)
+
+    # e2e: host buffers through the C-ABI host entry point
+    xh = torch.from_numpy(prob.x.copy()).pin_memory()
+    gh = torch.empty(x.numel(), dtype=torch.float64).pin_memory()
+    fh = ctypes.c_double(0.0)
+    e2e_ms = []
+    for it in range(args.warmup + args.steps):
+        flush.fill_(2.0)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        rc = L.necg_outprod_host(eng.h, prob.K, xh.data_ptr(), ctypes.addressof(fh), gh.data_ptr(),
+                                 stream.cuda_stream)
+        e1.record(stream)
+        _lib.check(rc, "necg_outprod_host")
+        e1.synchronize()
+        if it >= args.warmup:
+            e2e_ms.append(e0.elapsed_time(e1))
+    e2e_t = torch.tensor([sum(e2e_ms)], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
+    e2e_value = world * args.steps / (float(e2e_t.item()) * 1e-3)
+    assert abs(fh.value - E) <= 1e-12 * abs(E), (fh.value, E)
+    assert np.array_equal(gh.numpy(), g.cpu().numpy())
+
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+
+    K, nst, n = prob.K, prob.nst, prob.n
+    tf = term_flops(n)
+    grad_flops = K * K * nst * tf["grad"]
+    energy_flops = (K * (K + 1) // 2) * nst * tf["energy"]
+    ph = np.array(phases)
+    ph_mean = ph.mean(axis=0)
+    grad_ms = float(ph_mean[3])
+    achieved = grad_flops / (grad_ms * 1e-3) / 1e12
+    traffic = None
+    tpath = os.path.join(HERE, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        try:
+            traffic = json.load(open(tpath)).get(f"grad_kernel_{args.workload}")
+        except (OSError, ValueError):
+            traffic = None
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_port_rate(prob, args.cpu_seconds)
+    out = {
+        "metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded, oldquit.dat layout; no public dataset exists)",
+        "config": {"workload": args.workload, "desc": WORKLOADS[args.workload],
+                   "pair_elements_per_eval": prob.pairs, "terms_per_eval": (prob.pairs + K * K) * nst,
+                   "l2": "flushed between steps by a 256 MiB write, not timed",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+        "pair_elements_per_s": value * prob.pairs,
+        "energy": E,
+        "phase_ms": dict(zip(PHASES, [round(float(v), 4) for v in ph_mean])),
+        "roofline": {"bound": "fp64", "kernel": f"grad_kernel<{n}>", "achieved": achieved, "peak": peak.value,
+                     "unit": "TFLOP/s", "frac": achieved / peak.value, "traffic": traffic,
+                     "peak_source": "measured now by the FP64 FMA probe (necg_fp64_peak); "
+                                    "MEASURED_PEAKS.json has no FP64 figure; nominal B200 FP64 = 37 TFLOP/s",
+                     "flops_per_launch": grad_flops, "flops_per_term": tf["grad"],
+                     "special_per_term": tf["grad_special"],
+                     "energy_kernel": {"achieved": energy_flops / (float(ph_mean[1]) * 1e-3) / 1e12,
+                                       "flops_per_launch": energy_flops},
+                     "whole_eval_tflops": (grad_flops + energy_flops) / (total_ms / args.steps * 1e-3) / 1e12},
+        "e2e": {"value": e2e_value, "unit": "evals/s", "h2d_bytes_per_step": int(prob.x.nbytes),
+                "d2h_bytes_per_step": int(prob.x.nbytes) + 8,
+                "path": "necg_outprod_host (pinned host x -> f, g)"},
+        "gpu_launches": 8 * args.steps,
+        "cpu_baseline": cpu,
+        "clocks": clk,
+    }
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_engine(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,140 @@
+/*
+ * necg.h -- C ABI of the B200 engine for the NECG energy-and-gradient path.
+ *
+ * Drop-in boundary for the reference Python package
+ * (MauricioCafiero/NBO_CorrelatedGaussians, directory python/).  Each entry
+ * point names the reference function it replaces.  All pointers named *_dev are
+ * CUDA device pointers, *_host are host pointers; every array is FP64,
+ * C-contiguous.  `stream` is a cudaStream_t passed as void* (NULL = legacy
+ * default stream).  Every function returns an NECG_* status code and never
+ * throws or aborts.
+ *
+ * Problem layout (the state python/read_input.py:16-157 loads into
+ * python/shared.py):
+ *   n      particles in internal coordinates (shared.ne), 1..6
+ *   nst    symmetry terms
+ *   K      basis functions (shared.M)
+ *   mass   n*n inverse-mass tensor, row-major
+ *   ncv    n+1 charges, reference nucleus first
+ *   scvv   nst symmetry weights, ALREADY divided by nst (read_input.py:141)
+ *   sml    nst*n*n coordinate maps, sml[s*n*n + i*n + j] = shared.sml[i, j, s]
+ *   sms    nst*3n*3n shift maps,    sms[s*9n*n + i*3n + j] = shared.sms[i, j, s]
+ *   iv     K*blk packed parameters, blk = n(n+1)/2 + 3n: per basis function
+ *          vech(L_k) column-major (python/utils.py:42-55), then s_k as x,y,z
+ *          per particle (python/matel.py:59-84)
+ *   x      [iv, C] of length K*blk + K (python/outprod.py:40-41)
+ *   g      gradient of length K*blk + K: [GRADA, GRADC] (python/make_grad.py:90)
+ */
+#ifndef NECG_H
+#define NECG_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    NECG_OK = 0,
+    NECG_ERR_ARG = 1,          /* bad argument (size, pointer, index) */
+    NECG_ERR_NOT_PD = 2,       /* A_k + A_l' not positive definite for some pair */
+    NECG_ERR_NONFINITE = 3,    /* a non-finite energy or gradient was produced */
+    NECG_ERR_CUDA = 4,         /* a CUDA runtime call failed */
+    NECG_ERR_ALLOC = 5,        /* device allocation failed */
+    NECG_ERR_UNSUPPORTED = 6,  /* particle count outside 1..6 */
+    NECG_ERR_CAPACITY = 7      /* K larger than the handle's K_max */
+};
+
+typedef struct necg_handle necg_handle;
+
+/* Create a handle for one particle system and symmetry set; allocates the
+ * device workspace for bases of up to K_max functions.  Host pointers.
+ * Replaces the module state set up by python/read_input.py:78-157. */
+int necg_create(int n, int nst, int K_max, double efs, const double *mass_host,
+                const double *ncv_host, const double *scvv_host, const double *sml_host,
+                const double *sms_host, necg_handle **out);
+
+/* Release a handle and its device workspace. */
+int necg_destroy(necg_handle *h);
+
+/* Bytes of device workspace the handle holds. */
+long long necg_workspace_bytes(const necg_handle *h);
+
+/* Ket-chunk widths of the energy tiles (>= 1) and gradient tiles (>= 4; the
+ * partial buffer is sized for K_max / 4 chunks).  Set by the autotuner;
+ * defaults are chosen per n. */
+int necg_set_tiles(necg_handle *h, int lc_energy, int lc_grad);
+
+/* One objective evaluation: python/outprod.py:20-76 outprod(x) -> (f, g),
+ * including make_grad (python/make_grad.py:18-90).  Device pointers; H_dev and
+ * S_dev (K*K) receive the symmetric matrices and may be NULL (workspace is used).
+ * Asynchronous on `stream`; the pair status is read by necg_status(). */
+int necg_outprod(necg_handle *h, int K, const double *x_dev, double *f_dev, double *g_dev,
+                 double *H_dev, double *S_dev, void *stream);
+
+/* Same as necg_outprod with host input and outputs: copies x to the device,
+ * evaluates, copies f and g back and synchronises the stream.  Returns the
+ * pair status of the evaluation. */
+int necg_outprod_host(necg_handle *h, int K, const double *x_host, double *f_host,
+                      double *g_host, void *stream);
+
+/* Energy only: H, S (and optionally the kinetic and Coulomb parts Kin, Pot,
+ * NULL to skip) and f = C^T H C / C^T S C when C_dev and f_dev are non-NULL.
+ * python/necg.py:36-58 (_build_matrices) and python/outprod.py:46-68. */
+int necg_build_matrices(necg_handle *h, int K, const double *iv_dev, const double *C_dev,
+                        double *H_dev, double *S_dev, double *Kin_dev, double *Pot_dev,
+                        double *f_dev, void *stream);
+
+/* python/make_grad.py:18-90 make_grad(eng, norm): gradient of the Rayleigh
+ * quotient for given energy and normalisation, with GRADC from the supplied
+ * H and S.  g_dev has K*blk + K entries. */
+int necg_make_grad(necg_handle *h, int K, const double *iv_dev, const double *C_dev,
+                   const double *H_dev, const double *S_dev, double eng, double norm,
+                   double *g_dev, void *stream);
+
+/* python/matel.py:28-210 matel(stf, ii, jj) for a batch of terms.
+ * terms_dev: nterms * 3 ints (stf, ii, jj), 1-based.  out_dev: nterms * 4
+ * doubles (ov, tk, ert, zht). */
+int necg_matel(necg_handle *h, int K, const double *iv_dev, int nterms, const int *terms_dev,
+               double *out_dev, void *stream);
+
+/* python/gradel.py:27-392 gradel(stf, ii, jj) for a batch of terms.
+ * tgvl_dev, tgvls_dev: nterms * blk doubles (dH and dS with respect to the bra
+ * block [vech(L_ii), s_ii]), doubled when ii == jj as the reference does. */
+int necg_gradel(necg_handle *h, int K, const double *iv_dev, int nterms, const int *terms_dev,
+                double *tgvl_dev, double *tgvls_dev, void *stream);
+
+/* python/utils.py:78-106 f0(z) and df0(z) on an array (either output may be NULL). */
+int necg_f0(const double *z_dev, int count, double *f_dev, double *df_dev, void *stream);
+
+/* Synchronise the handle's last stream and report the pair status of the most
+ * recent evaluation: NECG_OK, NECG_ERR_NOT_PD or NECG_ERR_NONFINITE; *bad_pair
+ * (may be NULL) receives the first failing pair as k*K + l, or -1. */
+int necg_status(necg_handle *h, long long *bad_pair);
+
+/* Phase timing: when enabled, necg_outprod records CUDA events on its stream
+ * at the boundaries of its five phases -- prep (bra + ket records), energy
+ * tiles, H C / S C + finalize, gradient tiles, gradient reduce.  Profiling aid
+ * with no counterpart in the reference (which only prints wall-clock,
+ * python/necg.py:119-123). */
+int necg_profile(necg_handle *h, int enable);
+
+/* Milliseconds of the five phases of the last profiled necg_outprod call
+ * (synchronises its stream).  ms must hold 5 doubles. */
+int necg_phase_ms(necg_handle *h, double *ms);
+
+/* Measure the FP64 FMA throughput of the current device (TFLOP/s, FMA = 2)
+ * with a register-only probe kernel: the denominator of the FP64 roofline.
+ * Measurement aid with no counterpart in the reference. */
+int necg_fp64_peak(int iters, double *tflops, void *stream);
+
+/* Human-readable text for a status code. */
+const char *necg_status_string(int code);
+
+/* Algorithmic FP64 operation count of one (k, l, P) term (FMA = 2, add/mul = 1,
+ * div/sqrt/rsqrt/exp = 1 each) for the energy kernel (which = 0) and the
+ * gradient kernel (which = 1); *special receives the div/sqrt/exp part. */
+long long necg_term_flops(int n, int which, long long *special);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* NECG_H */

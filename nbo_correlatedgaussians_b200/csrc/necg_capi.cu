@@ -1,0 +1,432 @@
+// necg_capi.cu -- the extern "C" boundary declared in include/necg.h.
+//
+// A handle owns one particle system's constants (mass, charges, symmetry set)
+// on the device plus the workspace one evaluation needs for bases of up to
+// K_max functions:
+//   bra   BraLayout<n>::size * K_max       per-basis data (structure of arrays)
+//   ket   KetLayout<n>::size * K_max * nst per-(l, P) ket records
+//   part  part_stride(n) * K_max * ceil(K_max / lc_grad)   gradient tile partials
+//   H, S  K_max^2 each (used when the caller passes no H/S)
+//   rows  2 K_max, scal 4, x/g staging for the host-pointer entry point
+// Nothing is allocated after necg_create, so every device-pointer entry point
+// is stream-ordered and capturable in a CUDA graph once tiles for K exist.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <vector>
+
+#include "necg_kernels.cuh"
+#include "necg_math.cuh"
+#include "../../include/necg.h"
+
+using necg::LaunchArgs;
+
+struct necg_handle {
+    int n, nst, K_max;
+    double efs;
+    std::vector<double> mass, ncv, scvv, sml, sms;
+    double *d_sml = nullptr, *d_sms = nullptr, *d_scvv = nullptr;
+    double *d_bra = nullptr, *d_ket = nullptr, *d_part = nullptr;
+    double *d_H = nullptr, *d_S = nullptr, *d_rows = nullptr, *d_scal = nullptr;
+    double *d_x = nullptr, *d_g = nullptr, *d_f = nullptr;
+    int *d_status = nullptr;
+    int2 *d_tiles = nullptr;
+    int tiles_cap = 0, tiles_K = -1, tiles_lc = -1, ntiles = 0;
+    int lc_e = 8, lc_g = 8, lc_g_alloc = 8;
+    int device = 0;
+    cudaStream_t last_stream = nullptr;
+    long long ws_bytes = 0;
+    bool profile = false;
+    cudaEvent_t ev[6] = {};
+};
+
+namespace {
+
+int cuda_fail(cudaError_t e) {
+    if (e == cudaSuccess) return NECG_OK;
+    return e == cudaErrorMemoryAllocation ? NECG_ERR_ALLOC : NECG_ERR_CUDA;
+}
+
+#define CK(x)                                  \
+    do {                                       \
+        cudaError_t _e = (x);                  \
+        if (_e != cudaSuccess) return cuda_fail(_e); \
+    } while (0)
+
+template <typename T> int dalloc(necg_handle *h, T **p, size_t count) {
+    size_t bytes = count * sizeof(T);
+    if (bytes == 0) bytes = 16;
+    cudaError_t e = cudaMalloc((void **)p, bytes);
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        return cuda_fail(e);
+    }
+    h->ws_bytes += (long long)bytes;
+    return NECG_OK;
+}
+
+void mark(necg_handle *h, int i, cudaStream_t st) {
+    if (h->profile) cudaEventRecord(h->ev[i], st);
+}
+
+void free_all(necg_handle *h) {
+    for (cudaEvent_t &e : h->ev)
+        if (e) cudaEventDestroy(e);
+    void *ptrs[] = {h->d_sml, h->d_sms, h->d_scvv, h->d_bra, h->d_ket, h->d_part, h->d_H,
+                    h->d_S, h->d_rows, h->d_scal, h->d_x, h->d_g, h->d_f, h->d_status,
+                    h->d_tiles};
+    for (void *p : ptrs)
+        if (p) cudaFree(p);
+}
+
+// Energy tiles over the lower triangle: (kb, lc) with lc * LC <= kb * 32 + 31.
+int ensure_tiles(necg_handle *h, int K, cudaStream_t st) {
+    if (h->tiles_K == K && h->tiles_lc == h->lc_e) return NECG_OK;
+    std::vector<int2> t;
+    const int nkb = (K + 31) / 32;
+    for (int kb = 0; kb < nkb; ++kb) {
+        const int kmax = kb * 32 + 31;
+        for (int lc = 0; lc * h->lc_e <= kmax && lc * h->lc_e < K; ++lc) t.push_back(make_int2(kb, lc));
+    }
+    if ((int)t.size() > h->tiles_cap) {
+        if (h->d_tiles) cudaFree(h->d_tiles);
+        h->d_tiles = nullptr;
+        CK(cudaMalloc((void **)&h->d_tiles, t.size() * sizeof(int2)));
+        h->tiles_cap = (int)t.size();
+    }
+    CK(cudaMemcpyAsync(h->d_tiles, t.data(), t.size() * sizeof(int2), cudaMemcpyHostToDevice, st));
+    CK(cudaStreamSynchronize(st));
+    h->tiles_K = K;
+    h->tiles_lc = h->lc_e;
+    h->ntiles = (int)t.size();
+    return NECG_OK;
+}
+
+LaunchArgs base_args(necg_handle *h, int K) {
+    LaunchArgs a;
+    memset(&a, 0, sizeof(a));
+    a.n = h->n;
+    a.K = K;
+    a.nst = h->nst;
+    a.efs = h->efs;
+    a.mass_h = h->mass.data();
+    a.ncv_h = h->ncv.data();
+    a.sml = h->d_sml;
+    a.sms = h->d_sms;
+    a.scvv = h->d_scvv;
+    a.bra = h->d_bra;
+    a.ket = h->d_ket;
+    a.tiles = h->d_tiles;
+    a.ntiles = h->ntiles;
+    a.LC_e = h->lc_e;
+    a.LC_g = h->lc_g;
+    a.rows = h->d_rows;
+    a.scal = h->d_scal;
+    a.part = h->d_part;
+    a.status = h->d_status;
+    a.lam = 1.0;
+    return a;
+}
+
+int check_K(necg_handle *h, int K) {
+    if (!h) return NECG_ERR_ARG;
+    if (K < 1) return NECG_ERR_ARG;
+    if (K > h->K_max) return NECG_ERR_CAPACITY;
+    return NECG_OK;
+}
+
+int begin(necg_handle *h, cudaStream_t st) {
+    CK(cudaSetDevice(h->device));
+    h->last_stream = st;
+    necg::launch_reset_status(h->d_status, st);  // status = {0, INT_MAX}
+    return NECG_OK;
+}
+
+int finish_launch() {
+    cudaError_t e = cudaGetLastError();
+    return cuda_fail(e);
+}
+
+}  // namespace
+
+extern "C" {
+
+int necg_create(int n, int nst, int K_max, double efs, const double *mass_host,
+                const double *ncv_host, const double *scvv_host, const double *sml_host,
+                const double *sms_host, necg_handle **out) {
+    if (!out) return NECG_ERR_ARG;
+    *out = nullptr;
+    if (n < 1 || n > 6) return NECG_ERR_UNSUPPORTED;
+    if (nst < 1 || K_max < 1 || !mass_host || !ncv_host || !scvv_host || !sml_host || !sms_host)
+        return NECG_ERR_ARG;
+    necg_handle *h = new necg_handle();
+    h->n = n;
+    h->nst = nst;
+    h->K_max = K_max;
+    h->efs = efs;
+    h->mass.assign(mass_host, mass_host + n * n);
+    h->ncv.assign(ncv_host, ncv_host + n + 1);
+    h->scvv.assign(scvv_host, scvv_host + nst);
+    h->sml.assign(sml_host, sml_host + (size_t)nst * n * n);
+    h->sms.assign(sms_host, sms_host + (size_t)nst * 9 * n * n);
+    // default tile widths per particle count
+    h->lc_e = n >= 5 ? 4 : 8;
+    h->lc_g = n >= 5 ? 4 : 8;
+    h->lc_g_alloc = 1;  // partial buffer sized for the narrowest gradient tile
+    cudaGetDevice(&h->device);
+    const size_t K = (size_t)K_max;
+    const size_t blk = (size_t)(n * (n + 1) / 2 + 3 * n);
+    int rc = NECG_OK;
+    if (!rc) rc = dalloc(h, &h->d_sml, h->sml.size());
+    if (!rc) rc = dalloc(h, &h->d_sms, h->sms.size());
+    if (!rc) rc = dalloc(h, &h->d_scvv, (size_t)nst);
+    if (!rc) rc = dalloc(h, &h->d_bra, (size_t)necg::bra_record_size(n) * K);
+    if (!rc) rc = dalloc(h, &h->d_ket, (size_t)necg::ket_record_size(n) * K * nst);
+    if (!rc) rc = dalloc(h, &h->d_part, (size_t)necg::part_stride(n) * K * ((K + 3) / 4));
+    if (!rc) rc = dalloc(h, &h->d_H, K * K);
+    if (!rc) rc = dalloc(h, &h->d_S, K * K);
+    if (!rc) rc = dalloc(h, &h->d_rows, 2 * K);
+    if (!rc) rc = dalloc(h, &h->d_scal, (size_t)4);
+    if (!rc) rc = dalloc(h, &h->d_x, K * blk + K);
+    if (!rc) rc = dalloc(h, &h->d_g, K * blk + K);
+    if (!rc) rc = dalloc(h, &h->d_f, (size_t)2);
+    if (!rc) rc = dalloc(h, &h->d_status, (size_t)4);
+    if (!rc) rc = cuda_fail(cudaMemcpy(h->d_sml, h->sml.data(), h->sml.size() * 8, cudaMemcpyHostToDevice));
+    if (!rc) rc = cuda_fail(cudaMemcpy(h->d_sms, h->sms.data(), h->sms.size() * 8, cudaMemcpyHostToDevice));
+    if (!rc) rc = cuda_fail(cudaMemcpy(h->d_scvv, h->scvv.data(), h->scvv.size() * 8, cudaMemcpyHostToDevice));
+    if (!rc) rc = cuda_fail(cudaMemset(h->d_status, 0, 16));
+    if (rc) {
+        free_all(h);
+        delete h;
+        return rc;
+    }
+    *out = h;
+    return NECG_OK;
+}
+
+int necg_destroy(necg_handle *h) {
+    if (!h) return NECG_ERR_ARG;
+    cudaSetDevice(h->device);
+    free_all(h);
+    delete h;
+    return NECG_OK;
+}
+
+long long necg_workspace_bytes(const necg_handle *h) { return h ? h->ws_bytes : -1; }
+
+int necg_set_tiles(necg_handle *h, int lc_energy, int lc_grad) {
+    if (!h || lc_energy < 1 || lc_grad < 4 || lc_energy > 4096 || lc_grad > 4096)
+        return NECG_ERR_ARG;
+    h->lc_e = lc_energy;
+    h->lc_g = lc_grad;
+    return NECG_OK;
+}
+
+int necg_build_matrices(necg_handle *h, int K, const double *iv_dev, const double *C_dev,
+                        double *H_dev, double *S_dev, double *Kin_dev, double *Pot_dev,
+                        double *f_dev, void *stream) {
+    int rc = check_K(h, K);
+    if (rc) return rc;
+    if (!iv_dev) return NECG_ERR_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    if ((rc = begin(h, st))) return rc;
+    if ((rc = ensure_tiles(h, K, st))) return rc;
+    LaunchArgs a = base_args(h, K);
+    a.iv = iv_dev;
+    a.C = C_dev;
+    a.H = H_dev ? H_dev : h->d_H;
+    a.S = S_dev ? S_dev : h->d_S;
+    a.Kin = Kin_dev;
+    a.Pot = Pot_dev;
+    if (necg::launch_prep(a, st)) return NECG_ERR_UNSUPPORTED;
+    necg::launch_energy(a, st);
+    if (C_dev && f_dev) necg::launch_rows_finalize(a, f_dev, nullptr, 0, 0.0, 0.0, st);
+    return finish_launch();
+}
+
+int necg_outprod(necg_handle *h, int K, const double *x_dev, double *f_dev, double *g_dev,
+                 double *H_dev, double *S_dev, void *stream) {
+    int rc = check_K(h, K);
+    if (rc) return rc;
+    if (!x_dev || !g_dev) return NECG_ERR_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    if ((rc = begin(h, st))) return rc;
+    if ((rc = ensure_tiles(h, K, st))) return rc;
+    const size_t siv = (size_t)K * (h->n * (h->n + 1) / 2 + 3 * h->n);
+    LaunchArgs a = base_args(h, K);
+    a.iv = x_dev;
+    a.C = x_dev + siv;
+    a.H = H_dev ? H_dev : h->d_H;
+    a.S = S_dev ? S_dev : h->d_S;
+    a.g = g_dev;
+    mark(h, 0, st);
+    if (necg::launch_prep(a, st)) return NECG_ERR_UNSUPPORTED;
+    mark(h, 1, st);
+    necg::launch_energy(a, st);
+    mark(h, 2, st);
+    necg::launch_rows_finalize(a, f_dev, g_dev + siv, 0, 0.0, 0.0, st);
+    mark(h, 3, st);
+    necg::launch_grad_tiles(a, st);
+    mark(h, 4, st);
+    necg::launch_grad_reduce(a, st);
+    mark(h, 5, st);
+    return finish_launch();
+}
+
+int necg_outprod_host(necg_handle *h, int K, const double *x_host, double *f_host,
+                      double *g_host, void *stream) {
+    int rc = check_K(h, K);
+    if (rc) return rc;
+    if (!x_host || !g_host) return NECG_ERR_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    CK(cudaSetDevice(h->device));
+    const size_t len = (size_t)K * (h->n * (h->n + 1) / 2 + 3 * h->n) + K;
+    CK(cudaMemcpyAsync(h->d_x, x_host, len * sizeof(double), cudaMemcpyHostToDevice, st));
+    rc = necg_outprod(h, K, h->d_x, h->d_f, h->d_g, nullptr, nullptr, stream);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(g_host, h->d_g, len * sizeof(double), cudaMemcpyDeviceToHost, st));
+    if (f_host) CK(cudaMemcpyAsync(f_host, h->d_f, sizeof(double), cudaMemcpyDeviceToHost, st));
+    return necg_status(h, nullptr);
+}
+
+int necg_make_grad(necg_handle *h, int K, const double *iv_dev, const double *C_dev,
+                   const double *H_dev, const double *S_dev, double eng, double norm,
+                   double *g_dev, void *stream) {
+    int rc = check_K(h, K);
+    if (rc) return rc;
+    if (!iv_dev || !C_dev || !H_dev || !S_dev || !g_dev) return NECG_ERR_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    if ((rc = begin(h, st))) return rc;
+    const size_t siv = (size_t)K * (h->n * (h->n + 1) / 2 + 3 * h->n);
+    LaunchArgs a = base_args(h, K);
+    a.iv = iv_dev;
+    a.C = C_dev;
+    a.H = const_cast<double *>(H_dev);
+    a.S = const_cast<double *>(S_dev);
+    a.g = g_dev;
+    if (necg::launch_prep(a, st)) return NECG_ERR_UNSUPPORTED;
+    // GRADC = 2 norm (H - eng S) C with the caller's eng and norm; also sets
+    // the E and norm the gradient tiles read
+    necg::launch_rows_finalize(a, nullptr, g_dev + siv, 1, eng, norm, st);
+    necg::launch_grad(a, st);
+    return finish_launch();
+}
+
+int necg_matel(necg_handle *h, int K, const double *iv_dev, int nterms, const int *terms_dev,
+               double *out_dev, void *stream) {
+    int rc = check_K(h, K);
+    if (rc) return rc;
+    if (!iv_dev || nterms < 0 || (nterms > 0 && (!terms_dev || !out_dev))) return NECG_ERR_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    if ((rc = begin(h, st))) return rc;
+    LaunchArgs a = base_args(h, K);
+    a.iv = iv_dev;
+    a.C = nullptr;
+    if (necg::launch_prep(a, st)) return NECG_ERR_UNSUPPORTED;
+    if (nterms > 0) necg::launch_matel(a, terms_dev, nterms, out_dev, st);
+    return finish_launch();
+}
+
+int necg_gradel(necg_handle *h, int K, const double *iv_dev, int nterms, const int *terms_dev,
+                double *tgvl_dev, double *tgvls_dev, void *stream) {
+    int rc = check_K(h, K);
+    if (rc) return rc;
+    if (!iv_dev || nterms < 0 || (nterms > 0 && (!terms_dev || !tgvl_dev || !tgvls_dev)))
+        return NECG_ERR_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    if ((rc = begin(h, st))) return rc;
+    LaunchArgs a = base_args(h, K);
+    a.iv = iv_dev;
+    a.C = nullptr;
+    if (necg::launch_prep(a, st)) return NECG_ERR_UNSUPPORTED;
+    if (nterms > 0) necg::launch_gradel(a, terms_dev, nterms, tgvl_dev, tgvls_dev, st);
+    return finish_launch();
+}
+
+int necg_f0(const double *z_dev, int count, double *f_dev, double *df_dev, void *stream) {
+    if (count < 0 || (count > 0 && !z_dev)) return NECG_ERR_ARG;
+    if (count == 0) return NECG_OK;
+    necg::launch_f0(z_dev, count, f_dev, df_dev, (cudaStream_t)stream);
+    return finish_launch();
+}
+
+int necg_status(necg_handle *h, long long *bad_pair) {
+    if (!h) return NECG_ERR_ARG;
+    CK(cudaSetDevice(h->device));
+    int st[2];
+    CK(cudaMemcpyAsync(st, h->d_status, sizeof(st), cudaMemcpyDeviceToHost, h->last_stream));
+    CK(cudaStreamSynchronize(h->last_stream));
+    if (bad_pair) *bad_pair = st[1] == 0x7fffffff ? -1 : (long long)st[1];
+    if (st[0] & 1) return NECG_ERR_NOT_PD;
+    if (st[0] & 2) return NECG_ERR_NONFINITE;
+    if (st[0] & 4) return NECG_ERR_ARG;
+    return NECG_OK;
+}
+
+int necg_profile(necg_handle *h, int enable) {
+    if (!h) return NECG_ERR_ARG;
+    CK(cudaSetDevice(h->device));
+    if (enable && !h->ev[0])
+        for (cudaEvent_t &e : h->ev) CK(cudaEventCreate(&e));
+    h->profile = enable != 0;
+    return NECG_OK;
+}
+
+int necg_phase_ms(necg_handle *h, double *ms) {
+    if (!h || !ms || !h->ev[0]) return NECG_ERR_ARG;
+    CK(cudaSetDevice(h->device));
+    CK(cudaEventSynchronize(h->ev[5]));
+    for (int i = 0; i < 5; ++i) {
+        float t = 0.f;
+        CK(cudaEventElapsedTime(&t, h->ev[i], h->ev[i + 1]));
+        ms[i] = t;
+    }
+    return NECG_OK;
+}
+
+int necg_fp64_peak(int iters, double *tflops, void *stream) {
+    if (iters < 1 || !tflops) return NECG_ERR_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    int dev = 0, sms = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const int blocks = sms * 8;
+    double *sink = nullptr;
+    CK(cudaMalloc((void **)&sink, blocks * sizeof(double)));
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    necg::launch_fp64_probe(blocks, iters / 4 + 1, sink, st);  // warm-up
+    cudaEventRecord(e0, st);
+    necg::launch_fp64_probe(blocks, iters, sink, st);
+    cudaEventRecord(e1, st);
+    cudaError_t e = cudaEventSynchronize(e1);
+    float ms = 0.f;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(sink);
+    if (e != cudaSuccess) return cuda_fail(e);
+    const double flops = 2.0 * 8.0 * (double)iters * blocks * 256.0;
+    *tflops = flops / (ms * 1e-3) / 1e12;
+    return NECG_OK;
+}
+
+const char *necg_status_string(int code) {
+    switch (code) {
+    case NECG_OK: return "ok";
+    case NECG_ERR_ARG: return "invalid argument";
+    case NECG_ERR_NOT_PD: return "A_k + A_l' is not positive definite for some basis pair";
+    case NECG_ERR_NONFINITE: return "non-finite energy or gradient";
+    case NECG_ERR_CUDA: return "CUDA runtime error";
+    case NECG_ERR_ALLOC: return "device allocation failed";
+    case NECG_ERR_UNSUPPORTED: return "unsupported particle count (1..6)";
+    case NECG_ERR_CAPACITY: return "K exceeds the handle's K_max";
+    default: return "unknown status";
+    }
+}
+
+}  // extern "C"

@@ -1,0 +1,139 @@
+// necg_count.cu -- algorithmic FP64 operation count of one (k, l, P) term.
+//
+// The term templates of necg_math.cuh are instantiated on the host with a
+// counting scalar: every add, subtract and multiply counts 1 (so a fused
+// multiply-add counts 2), every division, square root, reciprocal square root
+// and exponential counts 1 in a separate "special" tally.  Negation and
+// comparisons are free.  The count follows the Pade branch of F0 (the branch
+// all pairs of the synthetic workloads take) and excludes the per-basis and
+// per-(l, P) preparation, which is amortised over K terms.
+#include <math.h>
+#include <stdlib.h>
+
+#include <vector>
+
+#include "necg_math.cuh"
+#include "../../include/necg.h"
+
+namespace necg {
+
+struct CountCtx {
+    long long flops = 0, special = 0;
+};
+static CountCtx g_ctx;
+
+struct CD {
+    double v;
+    CD() : v(0.0) {}
+    CD(double x) : v(x) {}
+    CD &operator+=(const CD &o) { ++g_ctx.flops; v += o.v; return *this; }
+    CD &operator-=(const CD &o) { ++g_ctx.flops; v -= o.v; return *this; }
+    CD &operator*=(const CD &o) { ++g_ctx.flops; v *= o.v; return *this; }
+};
+inline CD operator+(CD a, CD b) { ++g_ctx.flops; return CD(a.v + b.v); }
+inline CD operator-(CD a, CD b) { ++g_ctx.flops; return CD(a.v - b.v); }
+inline CD operator*(CD a, CD b) { ++g_ctx.flops; return CD(a.v * b.v); }
+inline CD operator/(CD a, CD b) { ++g_ctx.special; return CD(a.v / b.v); }
+inline CD operator+(double a, CD b) { return CD(a) + b; }
+inline CD operator+(CD a, double b) { return a + CD(b); }
+inline CD operator-(double a, CD b) { return CD(a) - b; }
+inline CD operator-(CD a, double b) { return a - CD(b); }
+inline CD operator*(double a, CD b) { return CD(a) * b; }
+inline CD operator*(CD a, double b) { return a * CD(b); }
+inline CD operator-(CD a) { return CD(-a.v); }
+inline bool operator>(CD a, double b) { return a.v > b; }
+inline bool operator<=(CD a, double b) { return a.v <= b; }
+inline bool operator<=(CD a, CD b) { return a.v <= b.v; }
+inline CD sqrt(CD a) { ++g_ctx.special; return CD(::sqrt(a.v)); }
+inline CD rsqrt(CD a) { ++g_ctx.special; return CD(1.0 / ::sqrt(a.v)); }
+inline CD exp(CD a) { ++g_ctx.special; return CD(::exp(a.v)); }
+
+struct HostBra {
+    const double *p;
+    int K, k;
+    CD operator()(int f) const { return CD(p[(size_t)f * K + k]); }
+};
+struct HostKet {
+    const double *p;
+    CD operator[](int i) const { return CD(p[i]); }
+};
+
+// Build one bra record (K = 1) and one ket record from a well-conditioned pair.
+template <int N> void host_records(std::vector<double> &bra, std::vector<double> &ket) {
+    using BL = BraLayout<N>;
+    using KL = KetLayout<N>;
+    bra.assign(BL::size, 0.0);
+    ket.assign(KL::size, 0.0);
+    double A[tri(N)], Ap[tri(N)];
+    for (int i = 0; i < N; ++i)
+        for (int j = 0; j <= i; ++j) {
+            A[sx(i, j)] = (i == j) ? 1.0 + 0.1 * i : 0.05;
+            Ap[sx(i, j)] = (i == j) ? 0.8 + 0.2 * i : -0.03;
+        }
+    for (int t = 0; t < tri(N); ++t) {
+        bra[BL::A + t] = A[t];
+        bra[BL::Nk + t] = 0.5 * A[t];
+        bra[BL::L + t] = A[t];
+        ket[KL::Ap + t] = Ap[t];
+        ket[KL::Np + t] = 0.5 * Ap[t];
+    }
+    for (int t = 0; t < 3 * N; ++t) {
+        bra[BL::S + t] = 0.01 * (t + 1);
+        bra[BL::AS + t] = 0.02 * (t + 1);
+        ket[KL::Sp + t] = -0.01 * (t + 2);
+        ket[KL::ASp + t] = -0.015 * (t + 2);
+    }
+    for (int t = 0; t < N * N; ++t) ket[KL::AMp + t] = 0.01 * t;
+    bra[BL::i1] = 0.01;
+    bra[BL::pre] = 1.0;
+    bra[BL::tMA] = 2.0;
+    ket[KL::i2] = 0.02;
+    ket[KL::pre] = 1.0;
+    ket[KL::tMA] = 1.0;
+    ket[KL::w] = 1.0;
+    ket[KL::wC] = 1.0;
+}
+
+template <int N> void count_term(int which, long long &flops, long long &special) {
+    std::vector<double> bra, ket;
+    host_records<N>(bra, ket);
+    Consts<N> cs;
+    for (int i = 0; i < N * N; ++i) cs.M[i] = (i % (N + 1) == 0) ? 0.5 : 0.01;
+    for (int t = 0; t < tri(N); ++t) cs.cv[t] = 1.0;
+    for (int i = 0; i < N; ++i) cs.q[i] = -1.0;
+    cs.efs = 1e-4;
+    cs.sqrt8n = ::sqrt(::pow(8.0, N));
+    HostBra b{bra.data(), 1, 0};
+    HostKet kr{ket.data()};
+    g_ctx = CountCtx();
+    if (which == 0) {
+        CD ov, tau, rho, sig;
+        term_energy<N>(b, kr, cs, ov, tau, rho, sig);
+        // the energy kernel's per-term accumulation: h, s, kinetic, potential
+        CD w(1.0), h(0.0), s(0.0);
+        h += w * ov * (2.0 * tau + rho - sig);
+        s += w * ov;
+    } else {
+        CD accG[tri(N)], accS[3 * N], accD;
+        term_grad<N>(b, kr, cs, CD(1.0), CD(0.5), CD(1.0), accG, accD, accS);
+    }
+    flops = g_ctx.flops;
+    special = g_ctx.special;
+}
+
+}  // namespace necg
+
+extern "C" long long necg_term_flops(int n, int which, long long *special) {
+    long long f = 0, s = 0;
+    switch (n) {
+    case 1: necg::count_term<1>(which, f, s); break;
+    case 2: necg::count_term<2>(which, f, s); break;
+    case 3: necg::count_term<3>(which, f, s); break;
+    case 4: necg::count_term<4>(which, f, s); break;
+    case 5: necg::count_term<5>(which, f, s); break;
+    case 6: necg::count_term<6>(which, f, s); break;
+    default: return -1;
+    }
+    if (special) *special = s;
+    return f + s;
+}

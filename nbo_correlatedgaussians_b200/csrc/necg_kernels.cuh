@@ -1,0 +1,41 @@
+// necg_kernels.cuh -- launcher interface between the C-ABI layer and the kernels.
+#pragma once
+#include <cuda_runtime.h>
+
+namespace necg {
+
+struct LaunchArgs {
+    int n, K, nst;
+    double efs;
+    const double *mass_h, *ncv_h;          // host copies (folded into kernel constants)
+    const double *iv, *C;                  // device: packed parameters, coefficients
+    const double *sml, *sms, *scvv;        // device: symmetry set
+    double *bra, *ket;                     // device workspace: bra SoA, ket records
+    const int2 *tiles;                     // energy tile list (kb, lc)
+    int ntiles, LC_e, LC_g;
+    double *H, *S, *Kin, *Pot;             // device outputs (Kin/Pot optional)
+    double *rows, *scal, *part, *g;        // device workspace / outputs
+    double lam, scale_override;
+    int *status;
+};
+
+int launch_prep(const LaunchArgs &a, cudaStream_t st);
+int launch_energy(const LaunchArgs &a, cudaStream_t st);
+int launch_grad(const LaunchArgs &a, cudaStream_t st);
+int launch_grad_tiles(const LaunchArgs &a, cudaStream_t st);
+int launch_grad_reduce(const LaunchArgs &a, cudaStream_t st);
+int launch_matel(const LaunchArgs &a, const int *terms, int nterms, double *out, cudaStream_t st);
+int launch_gradel(const LaunchArgs &a, const int *terms, int nterms, double *tg, double *tgs,
+                  cudaStream_t st);
+void launch_rows_finalize(const LaunchArgs &a, double *f_out, double *gradc, int given,
+                          double eng, double norm, cudaStream_t st);
+void launch_reset_status(int *status, cudaStream_t st);
+void launch_fp64_probe(int blocks, int iters, double *sink, cudaStream_t st);
+void launch_f0(const double *z, int count, double *f, double *df, cudaStream_t st);
+
+// sizes in doubles
+int ket_record_size(int n);
+int bra_record_size(int n);
+int part_stride(int n);
+
+}  // namespace necg

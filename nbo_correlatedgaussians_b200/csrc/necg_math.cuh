@@ -1,0 +1,519 @@
+// necg_math.cuh -- per-term FP64 math of the ECG energy+gradient path.
+//
+// One "term" is a (bra k, ket l, symmetry P) triple: the reference's
+// matel(stf, k, l) (python/matel.py:28-210) and the bra part of
+// gradel(stf, k, l) (python/gradel.py:27-392).  The reference expands every
+// n x n matrix to 3n x 3n with kron(., I3) and inverts with LAPACK; here all
+// work stays in n-space with the shifts viewed as n x 3 matrices, B = A_k + A_l'
+// is factored by Cholesky in registers, and the gradient is formed with respect
+// to A_k = L_k L_k^T (a symmetric n x n matrix) and s_k, then mapped to vech(L_k)
+// once per basis function (dF/dL = 2 G L).
+//
+// Notation (n = N particles):
+//   A_k, A_l' = P^T A_l P    symmetric, packed lower (N(N+1)/2)
+//   S_k, S_l' = sms s_l      n x 3 (row = particle, column = x, y, z)
+//   B = A_k + A_l', Bi = B^-1, T = Bi (A_k S_k + A_l' S_l')   (st in the reference)
+//   Dk = S_k - T, Dl = T - S_l', Y = A_l' Dl (= A_k Dk)
+//   ov  = sqrt(8^n) (|L_k| |L_l|)^{3/2} / |B|^{3/2} exp(<E,T> - i1 - i2)
+//   tau = 3 tr(M X) - 2 <Y, M Y>, X = A_k Bi A_l',   tk = 2 ov tau
+//   rho = sum_v c_v F0(|v^T T|^2 / v^T Bi v) (v^T Bi v)^{-1/2}, ert = ov rho
+//   sig = efs sum_i q_i T[i,z],  zht = ov sig
+// Coulomb pairs v: e_q (nucleus-particle) or e_p - e_q (particle-particle),
+// c_v = 2 q_p q_q / sqrt(pi).
+//
+// Bra gradient of F = w (h - E ov) with h = tk + ert - zht:
+//   dF/dA_k = Fw (-Dk Dk^T - 1.5 Bi + 0.75 A_k^-1)
+//             + ovw (Bi (6 N_l' + W) Bi + Qk Dk^T + Dk Qk^T)
+//   dF/ds_k = -2 Fw Y + 2 ovw A_k Qk
+//   N_l' = A_l' M A_l',  Qk = Bi (Z' - 4 A_l' M Y),
+//   Z' = sum_v alpha_v v b_v^T - (efs/2) q e_z^T,  W = sum_v beta_v v v^T,
+//   alpha_v = c_v F0'(z) a^{-3/2},  beta_v = c_v a^{-3/2} (z F0'(z) + F0(z)/2).
+// The A_k^-1 term maps to vech as 1.5/L_ii on the diagonal only, so it is kept
+// as one scalar per basis function.
+//
+// All term functions are templates over the scalar type R and over the bra and
+// ket accessors.  The kernels instantiate them with R = double; the operation
+// counter in the C-ABI layer instantiates them with a counting scalar on the
+// host, so the algorithmic FLOP count is taken from this very code.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#ifdef __CUDACC__
+#define NECG_HD __host__ __device__ __forceinline__
+#else
+#define NECG_HD inline
+#endif
+
+namespace necg {
+
+__host__ __device__ constexpr int tri(int n) { return n * (n + 1) / 2; }
+// packed lower-triangular, row-major: (i, j) with i >= j
+__host__ __device__ constexpr int sx(int i, int j) {
+    return i >= j ? i * (i + 1) / 2 + j : j * (j + 1) / 2 + i;
+}
+
+// Pade coefficients of the Boys function F0 (python/shared.py:76-86,
+// source/error_function_approximation.f90) and its branch point
+// (python/utils.py:85).
+#define NECG_PC1 0.564691197e-04
+#define NECG_PC2 0.758433197e-03
+#define NECG_PC3 0.769838037e-02
+#define NECG_PC4 0.629344460e-01
+#define NECG_PC5 0.213271302e+00
+#define NECG_PC6 0.720266520e-04
+#define NECG_PC7 0.955528842e-03
+#define NECG_PC8 0.101431553e-01
+#define NECG_PC9 0.738522953e-01
+#define NECG_PC10 0.338450368e+00
+#define NECG_PC11 0.879937801e+00
+#define NECG_F0_SPLIT 16.3578
+#define NECG_PI 3.141592653589793
+#define NECG_SQRT_PI 1.7724538509055159
+
+// Ket record: one per (l, P), read warp-uniformly by the tile kernels.
+// Layout (doubles): Ap[tri] Sp[3N] ASp[3N] Np[tri] AMp[N*N] i2 pre tMA w wC pad
+template <int N> struct KetLayout {
+    static constexpr int T = tri(N);
+    static constexpr int Ap = 0;
+    static constexpr int Sp = Ap + T;
+    static constexpr int ASp = Sp + 3 * N;
+    static constexpr int Np = ASp + 3 * N;
+    static constexpr int AMp = Np + T;
+    static constexpr int i2 = AMp + N * N;
+    static constexpr int pre = i2 + 1;
+    static constexpr int tMA = pre + 1;  // tr(M A_l')
+    static constexpr int w = tMA + 1;    // symmetry weight scvv[P]
+    static constexpr int wC = w + 1;     // 2 scvv[P] C_l (gradient weight)
+    static constexpr int size = (wC + 1 + 1) & ~1;  // even, 16-byte records
+};
+
+// Bra record: structure of arrays over k, field f of basis k at f*K + k.
+template <int N> struct BraLayout {
+    static constexpr int T = tri(N);
+    static constexpr int A = 0;
+    static constexpr int S = A + T;
+    static constexpr int AS = S + 3 * N;
+    static constexpr int Nk = AS + 3 * N;  // A_k M A_k
+    static constexpr int i1 = Nk + T;
+    static constexpr int pre = i1 + 1;
+    static constexpr int tMA = pre + 1;
+    static constexpr int L = tMA + 1;      // L_k, packed lower
+    static constexpr int size = L + T;
+};
+
+// Per-problem constants, passed to kernels by value (constant bank).
+template <int N> struct Consts {
+    double M[N * N];    // inverse-mass tensor, row-major
+    double cv[tri(N)];  // c_v for the n(n+1)/2 Coulomb pairs (p<q, q-major order)
+    double q[N];        // ncv[1..n]
+    double efs;
+    double sqrt8n;      // sqrt(8^n)
+};
+
+// Coulomb pair enumeration order: for q = 1..N, p = 0..q-1  -> index q(q-1)/2 + p
+__host__ __device__ constexpr int vidx(int p, int q) { return q * (q - 1) / 2 + p; }
+
+// ---------------------------------------------------------------------------
+// Device accessors
+#ifdef __CUDACC__
+// Bra fields are per-lane and invariant over a tile's ket loops; holding them in
+// registers would cost 2 (6N + 2 tri(N)) registers, so they are re-read from the
+// (L1-resident) structure-of-arrays at the point of use.  The volatile asm keeps
+// the compiler from hoisting the loads out of the ket loops.
+__device__ __forceinline__ double ldv(const double *p) {
+    double v;
+    asm volatile("ld.global.nc.f64 %0, [%1];" : "=d"(v) : "l"(p));
+    return v;
+}
+struct BraRef {
+    const double *p;  // bra + k
+    size_t K;
+    __device__ __forceinline__ double operator()(int f) const { return ldv(p + (size_t)f * K); }
+};
+#endif
+
+// ---------------------------------------------------------------------------
+// Cholesky of a packed SPD matrix B = R R^T; returns the inverse Bi (packed),
+// prod(1/R_ii) and a success flag.  Fully unrolled into registers.
+#pragma nv_exec_check_disable
+template <int N, typename R>
+NECG_HD bool chol_inverse(const R (&B)[tri(N)], R (&Bi)[tri(N)], R &prod_rinv) {
+    R Rm[tri(N)];
+    R rinv[N];
+    bool ok = true;
+#pragma unroll
+    for (int j = 0; j < N; ++j) {
+        R d = B[sx(j, j)];
+#pragma unroll
+        for (int k = 0; k < j; ++k) d -= Rm[sx(j, k)] * Rm[sx(j, k)];
+        const bool pos = d > 0.0;
+        ok = ok && pos;
+        if (!pos) d = R(1.0);
+        const R r = rsqrt(d);
+        rinv[j] = r;
+        Rm[sx(j, j)] = d * r;
+#pragma unroll
+        for (int i = j + 1; i < N; ++i) {
+            R s = B[sx(i, j)];
+#pragma unroll
+            for (int k = 0; k < j; ++k) s -= Rm[sx(i, k)] * Rm[sx(j, k)];
+            Rm[sx(i, j)] = s * r;
+        }
+    }
+    // W = R^-1 (lower triangular), in place
+#pragma unroll
+    for (int j = 0; j < N; ++j) {
+        Rm[sx(j, j)] = rinv[j];
+#pragma unroll
+        for (int i = j + 1; i < N; ++i) {
+            R s = Rm[sx(i, j)] * rinv[j];
+#pragma unroll
+            for (int k = j + 1; k < i; ++k) s += Rm[sx(i, k)] * Rm[sx(k, j)];
+            Rm[sx(i, j)] = -(s * rinv[i]);
+        }
+    }
+    // Bi = W^T W : Bi_ij = sum_{k >= max(i,j)} W_ki W_kj
+#pragma unroll
+    for (int i = 0; i < N; ++i)
+#pragma unroll
+        for (int j = 0; j <= i; ++j) {
+            R s = Rm[sx(i, i)] * Rm[sx(i, j)];
+#pragma unroll
+            for (int k = i + 1; k < N; ++k) s += Rm[sx(k, i)] * Rm[sx(k, j)];
+            Bi[sx(i, j)] = s;
+        }
+    R p = rinv[0];
+#pragma unroll
+    for (int j = 1; j < N; ++j) p *= rinv[j];
+    prod_rinv = p;
+    return ok;
+}
+
+// y = S x for S symmetric (packed, read through an accessor) and x n x 3
+#pragma nv_exec_check_disable
+template <int N, typename R, typename Acc>
+NECG_HD void symv3(const Acc &S, int off, const R (&x)[3 * N], R (&y)[3 * N]) {
+#pragma unroll
+    for (int i = 0; i < N; ++i)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            R s = S[off + sx(i, 0)] * x[c];
+#pragma unroll
+            for (int k = 1; k < N; ++k) s += S[off + sx(i, k)] * x[3 * k + c];
+            y[3 * i + c] = s;
+        }
+}
+
+// Boys-function pieces for one Coulomb pair.  Given a = v^T Bi v and
+// bb = |v^T T|^2 (z = bb / a) returns fs = F0(z) a^{-1/2} and, when GRAD,
+// dfs = F0'(z) a^{-1/2} and ia = 1/a.  The Pade branch (z <= 16.3578) and the
+// asymptotic branch sqrt(pi/(4z)) follow python/utils.py:78-106.
+#pragma nv_exec_check_disable
+template <bool GRAD, typename R>
+NECG_HD void boys(R a, R bb, R &fs, R &dfs, R &ia, R &z) {
+    ia = R(1.0) / a;
+    z = bb * ia;
+    if (z <= NECG_F0_SPLIT) {
+        const R num = ((((NECG_PC1 * z + NECG_PC2) * z + NECG_PC3) * z + NECG_PC4) * z +
+                       NECG_PC5) * z + 1.0;
+        const R den = (((((NECG_PC6 * z + NECG_PC7) * z + NECG_PC8) * z + NECG_PC9) * z +
+                        NECG_PC10) * z + NECG_PC11) * z + 1.0;
+        if (GRAD) {
+            const R nd = R(1.0) / (num * den);
+            const R r = num * num * nd;  // num / den
+            fs = sqrt(r * ia);
+            const R dN = (((5.0 * NECG_PC1 * z + 4.0 * NECG_PC2) * z + 3.0 * NECG_PC3) * z +
+                          2.0 * NECG_PC4) * z + NECG_PC5;
+            const R dD = ((((6.0 * NECG_PC6 * z + 5.0 * NECG_PC7) * z + 4.0 * NECG_PC8) * z +
+                           3.0 * NECG_PC9) * z + 2.0 * NECG_PC10) * z + NECG_PC11;
+            // F0' = (dN - r dD) / (2 den F0);  F0' a^-1/2 = (dN - r dD) fs / (2 num)
+            dfs = 0.5 * (dN - r * dD) * fs * (den * nd);
+        } else {
+            fs = sqrt(num * ia / den);
+            dfs = R(0.0);
+        }
+    } else {
+        // F0 = sqrt(pi / (4 z)) ; F0 a^-1/2 = sqrt(pi / (4 bb))
+        const R rb = rsqrt(bb);
+        fs = (0.5 * NECG_SQRT_PI) * rb;
+        if (GRAD) dfs = -0.5 * fs * a * rb * rb;  // F0' = -F0 / (2 z)
+        else dfs = R(0.0);
+    }
+}
+
+// B = A_k + A_l', its inverse, T = Bi (A_k S_k + A_l' S_l') and the overlap.
+#pragma nv_exec_check_disable
+template <int N, typename R, typename BA, typename KA>
+NECG_HD bool term_core(const BA &b, const KA &kr, const Consts<N> &cs, R (&Bi)[tri(N)],
+                       R (&T)[3 * N], R &ov) {
+    using KL = KetLayout<N>;
+    using BL = BraLayout<N>;
+    R prinv;
+    bool ok;
+    {
+        R B[tri(N)];
+#pragma unroll
+        for (int t = 0; t < tri(N); ++t) B[t] = b(BL::A + t) + kr[KL::Ap + t];
+        ok = chol_inverse<N>(B, Bi, prinv);
+    }
+    R Ev[3 * N];
+#pragma unroll
+    for (int t = 0; t < 3 * N; ++t) Ev[t] = b(BL::AS + t) + kr[KL::ASp + t];
+#pragma unroll
+    for (int i = 0; i < N; ++i)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            R s = Bi[sx(i, 0)] * Ev[c];
+#pragma unroll
+            for (int k = 1; k < N; ++k) s += Bi[sx(i, k)] * Ev[3 * k + c];
+            T[3 * i + c] = s;
+        }
+    R i3 = Ev[0] * T[0];
+#pragma unroll
+    for (int t = 1; t < 3 * N; ++t) i3 += Ev[t] * T[t];
+    const R p3 = prinv * prinv * prinv;
+    ov = cs.sqrt8n * b(BL::pre) * kr[KL::pre] * p3 * exp(i3 - b(BL::i1) - kr[KL::i2]);
+    return ok;
+}
+
+// tau = 3 tr(M X) - 2 <Y, M Y>.  tr(M X) with X = A_k Bi A_l' is written through
+// the matrix with the smaller tr(M A): X = A_s - A_s Bi A_s, which keeps the
+// subtraction free of cancellation.
+#pragma nv_exec_check_disable
+template <int N, typename R, typename BA, typename KA>
+NECG_HD R term_tau(const BA &b, const KA &kr, const Consts<N> &cs, const R (&Bi)[tri(N)],
+                   const R (&T)[3 * N]) {
+    using KL = KetLayout<N>;
+    using BL = BraLayout<N>;
+    R tMX;
+    {
+        const R tl = kr[KL::tMA], tk = b(BL::tMA);
+        R acc = R(0.0);
+        if (tl <= tk) {
+#pragma unroll
+            for (int i = 0; i < N; ++i)
+#pragma unroll
+                for (int j = 0; j <= i; ++j) {
+                    const R v = Bi[sx(i, j)] * kr[KL::Np + sx(i, j)];
+                    acc += (i == j) ? v : 2.0 * v;
+                }
+            tMX = tl - acc;
+        } else {
+#pragma unroll
+            for (int i = 0; i < N; ++i)
+#pragma unroll
+                for (int j = 0; j <= i; ++j) {
+                    const R v = Bi[sx(i, j)] * b(BL::Nk + sx(i, j));
+                    acc += (i == j) ? v : 2.0 * v;
+                }
+            tMX = tk - acc;
+        }
+    }
+    R yMy = R(0.0);
+    {
+        R Dl[3 * N], Y[3 * N];
+#pragma unroll
+        for (int t = 0; t < 3 * N; ++t) Dl[t] = T[t] - kr[KL::Sp + t];
+        symv3<N>(kr, KL::Ap, Dl, Y);
+#pragma unroll
+        for (int i = 0; i < N; ++i)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                R s = cs.M[i * N] * Y[c];
+#pragma unroll
+                for (int k = 1; k < N; ++k) s += cs.M[i * N + k] * Y[3 * k + c];
+                yMy += Y[3 * i + c] * s;
+            }
+    }
+    return 3.0 * tMX - 2.0 * yMy;
+}
+
+#pragma nv_exec_check_disable
+template <int N, typename R>
+NECG_HD R term_sig(const Consts<N> &cs, const R (&T)[3 * N]) {
+    R sg = cs.q[0] * T[2];
+#pragma unroll
+    for (int i = 1; i < N; ++i) sg += cs.q[i] * T[3 * i + 2];
+    return cs.efs * sg;
+}
+
+// Energy part: returns false if B is not positive definite.
+#pragma nv_exec_check_disable
+template <int N, typename R, typename BA, typename KA>
+NECG_HD bool term_energy(const BA &b, const KA &kr, const Consts<N> &cs, R &ov, R &tau, R &rho,
+                         R &sig) {
+    R Bi[tri(N)], T[3 * N];
+    const bool ok = term_core<N>(b, kr, cs, Bi, T, ov);
+    tau = term_tau<N>(b, kr, cs, Bi, T);
+    sig = term_sig<N>(cs, T);
+    // Coulomb sum (python/matel.py:162-197)
+    R r = R(0.0);
+#pragma unroll
+    for (int q = 1; q <= N; ++q)
+#pragma unroll
+        for (int p = 0; p < q; ++p) {
+            R a = Bi[sx(q - 1, q - 1)];
+            R bv[3];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) bv[c] = T[3 * (q - 1) + c];
+            if (p > 0) {
+                a += Bi[sx(p - 1, p - 1)] - 2.0 * Bi[sx(q - 1, p - 1)];
+#pragma unroll
+                for (int c = 0; c < 3; ++c) bv[c] -= T[3 * (p - 1) + c];
+            }
+            const R bb = bv[0] * bv[0] + bv[1] * bv[1] + bv[2] * bv[2];
+            R fs, dfs, ia, z;
+            boys<false>(a, bb, fs, dfs, ia, z);
+            r += cs.cv[vidx(p, q)] * fs;
+        }
+    rho = r;
+    return ok;
+}
+
+// Full term with bra gradient.  Fw = wgt (lam h - E ov), ovw = wgt lam ov:
+// lam = 1, E = current energy gives the gradient of H - E S (the optimiser's
+// combination); lam = 1, E = 0 gives dH alone; lam = 0, E = -1 gives dS alone.
+// accG: packed dF/dA_k, accD: coefficient of 0.75 A_k^-1, accS: dF/ds_k (n x 3).
+#pragma nv_exec_check_disable
+template <int N, typename R, typename BA, typename KA>
+NECG_HD bool term_grad(const BA &b, const KA &kr, const Consts<N> &cs, R lam, R E, R wgt,
+                       R (&accG)[tri(N)], R &accD, R (&accS)[3 * N]) {
+    using KL = KetLayout<N>;
+    using BL = BraLayout<N>;
+    R Bi[tri(N)], T[3 * N], ov;
+    const bool ok = term_core<N>(b, kr, cs, Bi, T, ov);
+    const R tau = term_tau<N>(b, kr, cs, Bi, T);
+    const R sig = term_sig<N>(cs, T);
+    // Coulomb with derivatives: rho, Z (n x 3), W (packed)
+    R Z[3 * N], W[tri(N)];
+#pragma unroll
+    for (int t = 0; t < 3 * N; ++t) Z[t] = R(0.0);
+#pragma unroll
+    for (int t = 0; t < tri(N); ++t) W[t] = R(0.0);
+    R rho = R(0.0);
+#pragma unroll
+    for (int q = 1; q <= N; ++q)
+#pragma unroll
+        for (int p = 0; p < q; ++p) {
+            R a = Bi[sx(q - 1, q - 1)];
+            R bv[3];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) bv[c] = T[3 * (q - 1) + c];
+            if (p > 0) {
+                a += Bi[sx(p - 1, p - 1)] - 2.0 * Bi[sx(q - 1, p - 1)];
+#pragma unroll
+                for (int c = 0; c < 3; ++c) bv[c] -= T[3 * (p - 1) + c];
+            }
+            const R bb = bv[0] * bv[0] + bv[1] * bv[1] + bv[2] * bv[2];
+            R fs, dfs, ia, z;
+            boys<true>(a, bb, fs, dfs, ia, z);
+            const double c = cs.cv[vidx(p, q)];
+            rho += c * fs;
+            const R al = c * dfs * ia;
+            const R be = c * ia * (dfs * z + 0.5 * fs);
+#pragma unroll
+            for (int cc = 0; cc < 3; ++cc) Z[3 * (q - 1) + cc] += al * bv[cc];
+            W[sx(q - 1, q - 1)] += be;
+            if (p > 0) {
+#pragma unroll
+                for (int cc = 0; cc < 3; ++cc) Z[3 * (p - 1) + cc] -= al * bv[cc];
+                W[sx(p - 1, p - 1)] += be;
+                W[sx(q - 1, p - 1)] -= be;
+            }
+        }
+    // Stark part of Z' (a per-problem constant column)
+#pragma unroll
+    for (int i = 0; i < N; ++i) Z[3 * i + 2] -= 0.5 * cs.efs * cs.q[i];
+    const R h = ov * (2.0 * tau + rho - sig);
+    const R Fw = wgt * (lam * h - E * ov);
+    const R ovw = wgt * lam * ov;
+    accD += 0.75 * Fw;
+    // accG += Bi (ovw (6 N_l' + W) - 1.5 Fw B) Bi,  B = A_k + A_l'
+    {
+        const R f15 = 1.5 * Fw;
+#pragma unroll
+        for (int t = 0; t < tri(N); ++t)
+            W[t] = ovw * (6.0 * kr[KL::Np + t] + W[t]) - f15 * (b(BL::A + t) + kr[KL::Ap + t]);
+#pragma unroll
+        for (int j = 0; j < N; ++j) {
+            R col[N];  // column j of W Bi
+#pragma unroll
+            for (int a = 0; a < N; ++a) {
+                R s = W[sx(a, 0)] * Bi[sx(0, j)];
+#pragma unroll
+                for (int k = 1; k < N; ++k) s += W[sx(a, k)] * Bi[sx(k, j)];
+                col[a] = s;
+            }
+#pragma unroll
+            for (int i = j; i < N; ++i) {
+                R s = Bi[sx(i, 0)] * col[0];
+#pragma unroll
+                for (int a = 1; a < N; ++a) s += Bi[sx(i, a)] * col[a];
+                accG[sx(i, j)] += s;
+            }
+        }
+    }
+    // Y = A_l' (T - S_l') ; Zk = Z' - 4 (A_l' M) Y ; Qk = Bi Zk
+    R Y[3 * N];
+    {
+        R Dl[3 * N];
+#pragma unroll
+        for (int t = 0; t < 3 * N; ++t) Dl[t] = T[t] - kr[KL::Sp + t];
+        symv3<N>(kr, KL::Ap, Dl, Y);
+    }
+#pragma unroll
+    for (int i = 0; i < N; ++i)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            R s = kr[KL::AMp + i * N] * Y[c];
+#pragma unroll
+            for (int k = 1; k < N; ++k) s += kr[KL::AMp + i * N + k] * Y[3 * k + c];
+            Z[3 * i + c] -= 4.0 * s;
+        }
+    R Q[3 * N];
+#pragma unroll
+    for (int i = 0; i < N; ++i)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            R s = Bi[sx(i, 0)] * Z[c];
+#pragma unroll
+            for (int k = 1; k < N; ++k) s += Bi[sx(i, k)] * Z[3 * k + c];
+            Q[3 * i + c] = s;
+        }
+    // accS += 2 ovw A_k Q - 2 Fw Y
+    {
+        const R o2 = 2.0 * ovw, f2 = 2.0 * Fw;
+#pragma unroll
+        for (int i = 0; i < N; ++i)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                R s = b(BL::A + sx(i, 0)) * Q[c];
+#pragma unroll
+                for (int k = 1; k < N; ++k) s += b(BL::A + sx(i, k)) * Q[3 * k + c];
+                accS[3 * i + c] += o2 * s - f2 * Y[3 * i + c];
+            }
+    }
+    // Rk = ovw Qk - Fw/2 Dk ; accG += Rk Dk^T + Dk Rk^T,  Dk = S_k - T
+    {
+        const R fh = 0.5 * Fw;
+#pragma unroll
+        for (int t = 0; t < 3 * N; ++t) {
+            const R dk = b(BL::S + t) - T[t];
+            T[t] = dk;
+            Q[t] = ovw * Q[t] - fh * dk;
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < N; ++i)
+#pragma unroll
+        for (int j = 0; j <= i; ++j) {
+            R s = Q[3 * i] * T[3 * j] + T[3 * i] * Q[3 * j];
+#pragma unroll
+            for (int c = 1; c < 3; ++c) s += Q[3 * i + c] * T[3 * j + c] + T[3 * i + c] * Q[3 * j + c];
+            accG[sx(i, j)] += s;
+        }
+    return ok;
+}
+
+}  // namespace necg

@@ -1,0 +1,194 @@
+"""Parity of the sm_100a kernels (through the C ABI) with the reference's golden
+vectors and with the CPU oracle.
+
+Tolerances: elements 1e-12 relative; E 1e-10 Eh absolute; gradients 1e-9
+relative norm-wise (max|g - g_ref| / max|g_ref|).
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+from oracle.oracle import Oracle  # noqa: E402
+from _util import TOL_E, TOL_ELEM, TOL_G, elem_rel, golden, normwise, problem_from  # noqa: E402
+
+
+@pytest.fixture(scope="module")
+def torch_cuda():
+    import torch
+    assert torch.cuda.is_available()
+    return torch
+
+
+def _engine(p, K_max=None):
+    from nbo_correlatedgaussians_b200.engine import Engine
+    return Engine(p, K_max=K_max or p.K)
+
+
+def test_f0_df0(torch_cuda):
+    from nbo_correlatedgaussians_b200.engine import boys_f0
+    d = golden("f0.npz")
+    f, df = boys_f0(d["z"])
+    assert np.max(np.abs(f - d["f0"]) / np.abs(d["f0"])) < 1e-14
+    assert np.max(np.abs(df - d["df0"]) / np.abs(d["df0"])) < 1e-13
+
+
+@pytest.mark.parametrize("system", ["He", "H2", "LiH"])
+def test_matel_gradel_elements(torch_cuda, system):
+    d = golden(f"elements_{system}.npz")
+    p = problem_from(d)
+    eng = _engine(p)
+    mat = eng.matel(p.iv, d["terms"])
+    err = elem_rel(mat, d["matel"], efs=p.efs)
+    assert err.max() < TOL_ELEM, err.max(axis=0)
+    tg, tgs = eng.gradel(p.iv, d["terms"])
+    assert normwise(tg, d["tgvl"]) < 1e-12
+    assert normwise(tgs, d["tgvls"]) < 1e-12
+
+
+def test_f0_branch_edge(torch_cuda):
+    d = golden("f0_edge.npz")
+    for tag in ("below", "above"):
+        p = problem_from(d, iv=d[f"iv_{tag}"])
+        eng = _engine(p)
+        m = eng.matel(p.iv, [(1, 2, 1)])
+        assert elem_rel(m, d[f"matel_{tag}"][None]).max() < TOL_ELEM
+        tg, tgs = eng.gradel(p.iv, [(1, 2, 1)])
+        assert normwise(tg[0], d[f"tgvl_{tag}"]) < 1e-12
+        assert normwise(tgs[0], d[f"tgvls_{tag}"]) < 1e-12
+
+
+@pytest.mark.parametrize("system", ["He", "H2", "LiH"])
+def test_outprod_golden(torch_cuda, system):
+    d = golden(f"outprod_{system}.npz")
+    p = problem_from(d)
+    f, g = _engine(p).outprod(p.x)
+    assert abs(f - float(d["E"])) < TOL_E
+    assert normwise(g, d["g"]) < TOL_G
+
+
+def test_oldquit_file_and_eigen_coefficients(torch_cuda):
+    d = golden("oldquit.npz")
+    p = problem_from(d)
+    eng = _engine(p)
+    f, g = eng.outprod(p.x)
+    assert abs(f - 4.296758204100342) < TOL_E
+    assert normwise(g, d["g"]) < TOL_G
+    f2, g2 = eng.outprod(np.concatenate([p.iv, d["C_eig"]]))
+    assert abs(f2 - (-7.023692395001888)) < TOL_E
+    assert normwise(g2, d["g_eig"]) < TOL_G
+    H, S, Kin, Pot, fb = eng.build_matrices(p.iv, p.C)
+    assert normwise(H.cpu().numpy(), d["H"]) < 1e-12
+    assert normwise(S.cpu().numpy(), d["S"]) < 1e-12
+    assert abs(float(fb.item()) - 4.296758204100342) < TOL_E
+
+
+@pytest.mark.parametrize("system,K", [("He", 64), ("H2", 64), ("LiH", 40)])
+def test_outprod_vs_oracle(torch_cuda, system, K):
+    from nbo_correlatedgaussians_b200 import synth
+    p = synth.make_problem(system, K, 100 + K)
+    p.C = np.random.default_rng(K).normal(size=K)  # general coefficients
+    fo, go, Ho, So = Oracle.from_problem(p).outprod(p.x, nthreads=8, return_hs=True)
+    eng = _engine(p)
+    f, g = eng.outprod(p.x)
+    assert abs(f - fo) < TOL_E
+    assert normwise(g, go) < TOL_G
+    H, S, Kin, Pot, _ = eng.build_matrices(p.iv)
+    assert normwise(H.cpu().numpy(), Ho) < 1e-12
+    assert normwise(S.cpu().numpy(), So) < 1e-12
+    Hk, Sk, Ko, Po = Oracle.from_problem(p).build_matrices(p.iv, nthreads=8)
+    assert normwise(Kin.cpu().numpy(), Ko) < 1e-12
+    assert normwise(Pot.cpu().numpy(), Po) < 1e-12
+
+
+def test_make_grad_matches_outprod_gradient(torch_cuda):
+    from nbo_correlatedgaussians_b200 import synth
+    p = synth.make_problem("H2", 48, 7)
+    eng = _engine(p)
+    f, g = eng.outprod(p.x)
+    H, S, _, _, _ = eng.build_matrices(p.iv, parts=False)
+    Hn, Sn = H.cpu().numpy(), S.cpu().numpy()
+    norm = 1.0 / float(p.C @ Sn @ p.C)
+    g2 = eng.make_grad(p.iv, p.C, Hn, Sn, f, norm).cpu().numpy()
+    assert normwise(g2, g) < 1e-13
+
+
+def test_drop_in_modules(torch_cuda, tmp_path):
+    """read_input -> matel / gradel / outprod / make_grad with the reference's
+    module-level calling convention."""
+    from nbo_correlatedgaussians_b200 import shared as sh
+    from nbo_correlatedgaussians_b200.gradel import gradel
+    from nbo_correlatedgaussians_b200.make_grad import make_grad
+    from nbo_correlatedgaussians_b200.matel import matel
+    from nbo_correlatedgaussians_b200.outprod import outprod
+    from nbo_correlatedgaussians_b200.problem import write_oldquit
+    from nbo_correlatedgaussians_b200.read_input import read_input
+    from nbo_correlatedgaussians_b200.utils import df0, f0
+    d = golden("oldquit.npz")
+    fn = tmp_path / "oldquit.dat"
+    write_oldquit(problem_from(d), str(fn))
+    read_input(str(fn))
+    e = golden("elements_LiH.npz")  # different basis: only check self-consistency here
+    x = np.concatenate([sh.iv, sh.C])
+    f, g = outprod(x)
+    assert abs(f - 4.296758204100342) < TOL_E and normwise(g, d["g"]) < TOL_G
+    assert normwise(sh.H, d["H"]) < 1e-12 and np.array_equal(sh.grad, g)
+    make_grad(f, 1.0 / float(sh.C @ sh.S @ sh.C))
+    assert normwise(sh.grad, g) < 1e-13
+    o = Oracle.from_problem(problem_from(d))
+    for t in [(1, 1, 1), (5, 3, 7), (24, 12, 4), (11, 6, 6)]:
+        ref = np.array(o.matel(sh.iv, *t))
+        assert elem_rel(np.array(matel(*t))[None], ref[None], efs=sh.efs).max() < TOL_ELEM
+        tg, tgs = gradel(*t)
+        rg, rgs = o.gradel(sh.iv, *t)
+        assert normwise(tg, rg) < 1e-12 and normwise(tgs, rgs) < 1e-12
+    assert abs(f0(0.5) - o.f0(0.5)) < 1e-15 and abs(df0(20.0) - o.df0(20.0)) < 1e-15
+    del e
+
+
+def test_full_size_properties(torch_cuda):
+    """LiH K=1024 (the benchmark workload): properties that hold at any size.
+    E is invariant under C -> a C, so g_C . C = 0; the directional derivative
+    of E along a random unit direction matches g . u (5-point stencil)."""
+    torch = torch_cuda
+    from nbo_correlatedgaussians_b200 import synth
+    p = synth.workload("lih_k1024")
+    eng = _engine(p)
+    x = torch.from_numpy(p.x).cuda()
+    f, g = eng.outprod_device(x, p.K)
+    eng.raise_status("outprod")
+    f = float(f.item())
+    g = g.cpu().numpy()
+    assert np.isfinite(f) and np.isfinite(g).all()
+    gC = g[p.siv:]
+    assert abs(gC @ p.C) < 1e-12 * np.abs(gC).sum() * np.abs(p.C).max() + 1e-15
+    f3, _ = eng.outprod_device(torch.from_numpy(np.concatenate([p.iv, 3.0 * p.C])).cuda(), p.K)
+    assert abs(float(f3.item()) - f) < 1e-12 * abs(f)
+    u = np.random.default_rng(0).normal(size=p.x.size)
+    u /= np.linalg.norm(u)
+    h = 1e-4
+    vals = []
+    for s in (-2, -1, 1, 2):
+        fs, _ = eng.outprod_device(torch.from_numpy(p.x + s * h * u).cuda(), p.K)
+        vals.append(float(fs.item()))
+    fd = (vals[0] - 8 * vals[1] + 8 * vals[2] - vals[3]) / (12 * h)
+    assert abs(fd - g @ u) < 1e-6 * max(abs(g @ u), np.abs(g).max())
+    # deterministic: the same call twice gives identical bits
+    f_a, g_a = eng.outprod_device(x, p.K)
+    f_b, g_b = eng.outprod_device(x, p.K)
+    assert torch.equal(g_a, g_b) and torch.equal(f_a, f_b)
+
+
+def test_errors(torch_cuda):
+    from nbo_correlatedgaussians_b200 import _lib, synth
+    p = synth.make_problem("He", 8, 3)
+    eng = _engine(p)
+    with pytest.raises(_lib.NecgError):
+        eng.outprod_device(np.zeros(9 * 9 + 9), 9)  # K > K_max
+    bad = p.copy()
+    bad.iv[2 * p.blk:2 * p.blk + p.svh] = 0.0  # L_3 = 0: A_3 + A_3' singular
+    with pytest.raises(np.linalg.LinAlgError):
+        eng.outprod(bad.x)
+    # the handle stays usable after the error
+    f, g = eng.outprod(p.x)
+    assert np.isfinite(f)
