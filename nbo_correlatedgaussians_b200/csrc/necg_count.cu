@@ -13,50 +13,10 @@
 #include <vector>
 
 #include "necg_math.cuh"
+#include "necg_hostscalar.cuh"
 #include "../../include/necg.h"
 
 namespace necg {
-
-struct CountCtx {
-    long long flops = 0, special = 0;
-};
-static CountCtx g_ctx;
-
-struct CD {
-    double v;
-    CD() : v(0.0) {}
-    CD(double x) : v(x) {}
-    CD &operator+=(const CD &o) { ++g_ctx.flops; v += o.v; return *this; }
-    CD &operator-=(const CD &o) { ++g_ctx.flops; v -= o.v; return *this; }
-    CD &operator*=(const CD &o) { ++g_ctx.flops; v *= o.v; return *this; }
-};
-inline CD operator+(CD a, CD b) { ++g_ctx.flops; return CD(a.v + b.v); }
-inline CD operator-(CD a, CD b) { ++g_ctx.flops; return CD(a.v - b.v); }
-inline CD operator*(CD a, CD b) { ++g_ctx.flops; return CD(a.v * b.v); }
-inline CD operator/(CD a, CD b) { ++g_ctx.special; return CD(a.v / b.v); }
-inline CD operator+(double a, CD b) { return CD(a) + b; }
-inline CD operator+(CD a, double b) { return a + CD(b); }
-inline CD operator-(double a, CD b) { return CD(a) - b; }
-inline CD operator-(CD a, double b) { return a - CD(b); }
-inline CD operator*(double a, CD b) { return CD(a) * b; }
-inline CD operator*(CD a, double b) { return a * CD(b); }
-inline CD operator-(CD a) { return CD(-a.v); }
-inline bool operator>(CD a, double b) { return a.v > b; }
-inline bool operator<=(CD a, double b) { return a.v <= b; }
-inline bool operator<=(CD a, CD b) { return a.v <= b.v; }
-inline CD sqrt(CD a) { ++g_ctx.special; return CD(::sqrt(a.v)); }
-inline CD rsqrt(CD a) { ++g_ctx.special; return CD(1.0 / ::sqrt(a.v)); }
-inline CD exp(CD a) { ++g_ctx.special; return CD(::exp(a.v)); }
-
-struct HostBra {
-    const double *p;
-    int K, k;
-    CD operator()(int f) const { return CD(p[(size_t)f * K + k]); }
-};
-struct HostKet {
-    const double *p;
-    CD operator[](int i) const { return CD(p[i]); }
-};
 
 // Build one bra record (K = 1) and one ket record from a well-conditioned pair.
 template <int N> void host_records(std::vector<double> &bra, std::vector<double> &ket) {
@@ -103,9 +63,9 @@ template <int N> void count_term(int which, long long &flops, long long &special
     for (int i = 0; i < N; ++i) cs.q[i] = -1.0;
     cs.efs = 1e-4;
     cs.sqrt8n = ::sqrt(::pow(8.0, N));
-    HostBra b{bra.data(), 1, 0};
+    HostBra b{bra.data(), 1};
     HostKet kr{ket.data()};
-    g_ctx = CountCtx();
+    count_ctx() = CountCtx();
     if (which == 0) {
         CD ov, tau, rho, sig;
         term_energy<N>(b, kr, cs, ov, tau, rho, sig);
@@ -117,8 +77,8 @@ template <int N> void count_term(int which, long long &flops, long long &special
         CD accG[tri(N)], accS[3 * N], accD;
         term_grad<N>(b, kr, cs, CD(1.0), CD(0.5), CD(1.0), accG, accD, accS);
     }
-    flops = g_ctx.flops;
-    special = g_ctx.special;
+    flops = count_ctx().flops;
+    special = count_ctx().special;
 }
 
 }  // namespace necg

@@ -28,8 +28,8 @@
 //   N_l' = A_l' M A_l',  Qk = Bi (Z' - 4 A_l' M Y),
 //   Z' = sum_v alpha_v v b_v^T - (efs/2) q e_z^T,  W = sum_v beta_v v v^T,
 //   alpha_v = c_v F0'(z) a^{-3/2},  beta_v = c_v a^{-3/2} (z F0'(z) + F0(z)/2).
-// The A_k^-1 term maps to vech as 1.5/L_ii on the diagonal only, so it is kept
-// as one scalar per basis function.
+// The A_k^-1 term (coefficient D = 0.75 Fw) maps to vech(dF/dL) as 2 D / L_ii
+// on the diagonal only, so it is kept as one scalar per basis function.
 //
 // All term functions are templates over the scalar type R and over the bra and
 // ket accessors.  The kernels instantiate them with R = double; the operation
@@ -374,7 +374,7 @@ NECG_HD bool term_energy(const BA &b, const KA &kr, const Consts<N> &cs, R &ov, 
 // Full term with bra gradient.  Fw = wgt (lam h - E ov), ovw = wgt lam ov:
 // lam = 1, E = current energy gives the gradient of H - E S (the optimiser's
 // combination); lam = 1, E = 0 gives dH alone; lam = 0, E = -1 gives dS alone.
-// accG: packed dF/dA_k, accD: coefficient of 0.75 A_k^-1, accS: dF/ds_k (n x 3).
+// accG: packed dF/dA_k, accD: coefficient of A_k^-1 in dF/dA_k, accS: dF/ds_k (n x 3).
 #pragma nv_exec_check_disable
 template <int N, typename R, typename BA, typename KA>
 NECG_HD bool term_grad(const BA &b, const KA &kr, const Consts<N> &cs, R lam, R E, R wgt,

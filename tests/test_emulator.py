@@ -1,0 +1,67 @@
+"""The kernels' per-thread bodies, run on the host by the test emulator
+(tests/emu), against the golden vectors and the oracle.  This checks the device
+algorithm -- tile and lane ranges, ket records, reductions, the A-space to
+vech(L) mapping -- on CPU; the GPU parity tests check the compiled kernels."""
+import numpy as np
+import pytest
+
+from emu import emu
+from oracle.oracle import Oracle
+from nbo_correlatedgaussians_b200 import synth
+from _util import TOL_E, TOL_ELEM, TOL_G, elem_rel, golden, normwise, problem_from
+
+
+@pytest.mark.parametrize("system", ["He", "H2", "LiH"])
+def test_elements_vs_golden(system):
+    d = golden(f"elements_{system}.npz")
+    p = problem_from(d)
+    rc, mat, tg, tgs = emu.elements(p, d["terms"])
+    assert rc == 0
+    assert elem_rel(mat, d["matel"], efs=p.efs).max() < TOL_ELEM
+    assert normwise(tg, d["tgvl"]) < 1e-12
+    assert normwise(tgs, d["tgvls"]) < 1e-12
+
+
+@pytest.mark.parametrize("system", ["He", "H2", "LiH"])
+def test_outprod_vs_golden(system):
+    d = golden(f"outprod_{system}.npz")
+    p = problem_from(d)
+    rc, f, g, H, S = emu.outprod(p)
+    assert rc == 0
+    assert abs(f - float(d["E"])) < TOL_E
+    assert normwise(g, d["g"]) < TOL_G
+    assert normwise(H, d["H"]) < 1e-12 and normwise(S, d["S"]) < 1e-12
+
+
+def test_oldquit():
+    d = golden("oldquit.npz")
+    p = problem_from(d)
+    rc, f, g, H, S = emu.outprod(p)
+    assert rc == 0 and abs(f - 4.296758204100342) < TOL_E and normwise(g, d["g"]) < TOL_G
+
+
+@pytest.mark.parametrize("system,K,lc_e,lc_g", [("He", 45, 1, 4), ("He", 45, 7, 5), ("H2", 37, 3, 9),
+                                                ("H2", 70, 8, 16), ("LiH", 33, 4, 4), ("LiH", 33, 64, 64)])
+def test_outprod_vs_oracle_ragged_tiles(system, K, lc_e, lc_g):
+    """K not a multiple of the warp width, tile widths that do not divide K."""
+    p = synth.make_problem(system, K, 7 * K)
+    p.C = np.random.default_rng(K).normal(size=K)
+    fo, go = Oracle.from_problem(p).outprod(p.x, nthreads=8)
+    rc, f, g, H, S = emu.outprod(p, lc_e, lc_g)
+    assert rc == 0
+    assert abs(f - fo) < TOL_E
+    assert normwise(g, go) < TOL_G
+
+
+def test_single_basis_function():
+    p = synth.make_problem("H2", 1, 3)
+    fo, go = Oracle.from_problem(p).outprod(p.x)
+    rc, f, g, H, S = emu.outprod(p, 1, 4)
+    assert rc == 0 and abs(f - fo) < TOL_E and normwise(g, go) < TOL_G
+
+
+def test_not_positive_definite_flag():
+    p = synth.make_problem("He", 5, 3)
+    p.iv[2 * p.blk:2 * p.blk + p.svh] = 0.0
+    rc, f, g, H, S = emu.outprod(p)
+    assert rc & 1

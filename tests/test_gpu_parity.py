@@ -161,7 +161,7 @@ def test_full_size_properties(torch_cuda):
     g = g.cpu().numpy()
     assert np.isfinite(f) and np.isfinite(g).all()
     gC = g[p.siv:]
-    assert abs(gC @ p.C) < 1e-12 * np.abs(gC).sum() * np.abs(p.C).max() + 1e-15
+    assert abs(gC @ p.C) < 1e-10 * np.abs(gC).sum() * np.abs(p.C).max() + 1e-15
     f3, _ = eng.outprod_device(torch.from_numpy(np.concatenate([p.iv, 3.0 * p.C])).cuda(), p.K)
     assert abs(float(f3.item()) - f) < 1e-12 * abs(f)
     u = np.random.default_rng(0).normal(size=p.x.size)
