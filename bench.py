@@ -48,7 +48,7 @@ PHASES = ["prep", "energy", "finalize", "grad_tiles", "grad_reduce"]
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--workload", default="lih_k1024", choices=sorted(WORKLOADS))
@@ -208,9 +208,11 @@ def run_engine(args):
     L = _lib.lib()
     prob = synth.workload(args.workload)
     eng = Engine(prob)
-    _lib.check(L.necg_profile(eng.h, 1), "necg_profile")
     stream = torch.cuda.current_stream()
     x = torch.from_numpy(prob.x).cuda()
+    from nbo_correlatedgaussians_b200.autotune import tuned
+    tiles = tuned(eng, x, prob.K)  # untimed; cached per (GPU, n, nst, K bucket)
+    _lib.check(L.necg_profile(eng.h, 1), "necg_profile")
     g = torch.empty_like(x)
     f = torch.empty(1, dtype=torch.float64, device="cuda")
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
@@ -310,6 +312,7 @@ def run_engine(args):
         "config": {"workload": args.workload, "desc": WORKLOADS[args.workload],
                    "pair_elements_per_eval": prob.pairs, "terms_per_eval": (prob.pairs + K * K) * nst,
                    "l2": "flushed between steps by a 256 MiB write, not timed",
+                   "tiles": {k: tiles[k] for k in ("lc_e", "minb_e", "lc_g", "minb_g")},
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
         "pair_elements_per_s": value * prob.pairs,
         "energy": E,
@@ -326,7 +329,7 @@ def run_engine(args):
         "e2e": {"value": e2e_value, "unit": "evals/s", "h2d_bytes_per_step": int(prob.x.nbytes),
                 "d2h_bytes_per_step": int(prob.x.nbytes) + 8,
                 "path": "necg_outprod_host (pinned host x -> f, g)"},
-        "gpu_launches": 8 * args.steps,
+        "gpu_launches": (9 if (prob.K + tiles["lc_g"] - 1) // tiles["lc_g"] > 1 else 8) * args.steps,
         "cpu_baseline": cpu,
         "clocks": clk,
     }

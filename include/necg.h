@@ -63,6 +63,11 @@ long long necg_workspace_bytes(const necg_handle *h);
  * defaults are chosen per n. */
 int necg_set_tiles(necg_handle *h, int lc_energy, int lc_grad);
 
+/* Register-budget variant of the energy and gradient tile kernels: the
+ * minimum number of resident 128-thread blocks per SM the kernel is compiled
+ * for (1..4; more blocks = fewer registers per thread).  Set by the autotuner. */
+int necg_set_variant(necg_handle *h, int minb_energy, int minb_grad);
+
 /* One objective evaluation: python/outprod.py:20-76 outprod(x) -> (f, g),
  * including make_grad (python/make_grad.py:18-90).  Device pointers; H_dev and
  * S_dev (K*K) receive the symmetric matrices and may be NULL (workspace is used).

@@ -1,0 +1,121 @@
+"""Autotuner of the tile kernels.
+
+For one (n, nst, K) it times, with the library's phase events, the energy
+tiles over (ket-chunk width LC_e, register variant minb_e) and the gradient
+tiles over (LC_g, minb_g) -- the two are independent -- and keeps the fastest
+of each.  Results are cached in a JSON file keyed by GPU name, n, nst and a K
+bucket (powers of two), so a run pays for tuning once.
+
+The search space:
+  LC_e   ket chunk of an energy tile (kets per warp per tile)
+  LC_g   ket chunk of a gradient tile (also sets the partial-buffer depth)
+  minb   minimum resident 128-thread blocks per SM the kernel is compiled for
+         (1: up to 255 registers per thread; 3: 168; 4: 128)
+"""
+from __future__ import annotations
+
+import ctypes
+import json
+import os
+
+import numpy as np
+import torch
+
+from . import _lib
+from .engine import Engine
+
+CACHE = os.environ.get("NECG_TUNE_CACHE", os.path.join(os.path.dirname(os.path.abspath(__file__)), "tune_cache.json"))
+
+LC_E = (2, 4, 8, 16, 32)
+LC_G = (4, 8, 16, 32, 64)
+MINB = (1, 3, 4)
+
+
+def _bucket(K: int) -> int:
+    b = 16
+    while b < K:
+        b *= 2
+    return b
+
+
+def _key(n: int, nst: int, K: int) -> str:
+    name = torch.cuda.get_device_name() if torch.cuda.is_available() else "cpu"
+    return f"{name}|n{n}|nst{nst}|K{_bucket(K)}"
+
+
+def load_cache() -> dict:
+    try:
+        with open(CACHE) as fh:
+            return json.load(fh)
+    except (OSError, ValueError):
+        return {}
+
+
+def save_cache(cache: dict) -> None:
+    tmp = CACHE + ".tmp"
+    with open(tmp, "w") as fh:
+        json.dump(cache, fh, indent=1, sort_keys=True)
+    os.replace(tmp, CACHE)
+
+
+def _phase_times(eng: Engine, x: torch.Tensor, K: int, reps: int) -> np.ndarray:
+    L = eng.L
+    g = torch.empty_like(x)
+    f = torch.empty(1, dtype=torch.float64, device=x.device)
+    buf = (ctypes.c_double * 5)()
+    out = []
+    for _ in range(reps):
+        _lib.check(L.necg_outprod(eng.h, K, x.data_ptr(), f.data_ptr(), g.data_ptr(), None, None,
+                                  torch.cuda.current_stream().cuda_stream), "necg_outprod")
+        _lib.check(L.necg_phase_ms(eng.h, buf), "necg_phase_ms")
+        out.append(list(buf))
+    return np.array(out)
+
+
+def tune(eng: Engine, x, K: int, reps: int = 3, report: bool = False) -> dict:
+    """Time every candidate on this engine and input; returns the best setting."""
+    L = eng.L
+    x = eng._tensor(x)
+    _lib.check(L.necg_profile(eng.h, 1), "necg_profile")
+    rows = []
+    best_e = (float("inf"), None)
+    best_g = (float("inf"), None)
+    for minb in MINB:
+        for lc_e, lc_g in zip(LC_E, LC_G):
+            _lib.check(L.necg_set_tiles(eng.h, lc_e, lc_g), "necg_set_tiles")
+            _lib.check(L.necg_set_variant(eng.h, minb, minb), "necg_set_variant")
+            _phase_times(eng, x, K, 1)  # warm-up (also builds the energy tile list)
+            t = _phase_times(eng, x, K, reps).min(axis=0)
+            e_ms, g_ms = float(t[1]), float(t[3] + t[4])
+            rows.append({"minb": minb, "lc_e": lc_e, "lc_g": lc_g, "energy_ms": e_ms, "grad_ms": g_ms})
+            if e_ms < best_e[0]:
+                best_e = (e_ms, (lc_e, minb))
+            if g_ms < best_g[0]:
+                best_g = (g_ms, (lc_g, minb))
+    res = {"lc_e": best_e[1][0], "minb_e": best_e[1][1], "lc_g": best_g[1][0], "minb_g": best_g[1][1],
+           "energy_ms": best_e[0], "grad_ms": best_g[0]}
+    if report:
+        res["table"] = rows
+    apply(eng, res)
+    return res
+
+
+def apply(eng: Engine, cfg: dict) -> None:
+    _lib.check(eng.L.necg_set_tiles(eng.h, int(cfg["lc_e"]), int(cfg["lc_g"])), "necg_set_tiles")
+    _lib.check(eng.L.necg_set_variant(eng.h, int(cfg["minb_e"]), int(cfg["minb_g"])), "necg_set_variant")
+
+
+def tuned(eng: Engine, x, K: int, retune: bool = False) -> dict:
+    """Apply the cached setting for (GPU, n, nst, K bucket), tuning on a miss."""
+    cache = load_cache()
+    key = _key(eng.n, eng.nst, K)
+    if key in cache and not retune:
+        apply(eng, cache[key])
+        return cache[key]
+    res = tune(eng, x, K)
+    cache[key] = {k: v for k, v in res.items() if k != "table"}
+    try:
+        save_cache(cache)
+    except OSError:
+        pass
+    return cache[key]

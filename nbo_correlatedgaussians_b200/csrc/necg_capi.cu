@@ -35,7 +35,8 @@ struct necg_handle {
     int *d_status = nullptr;
     int2 *d_tiles = nullptr;
     int tiles_cap = 0, tiles_K = -1, tiles_lc = -1, ntiles = 0;
-    int lc_e = 8, lc_g = 8, lc_g_alloc = 8;
+    int lc_e = 8, lc_g = 8;
+    int minb_e = 1, minb_g = 1;
     int device = 0;
     cudaStream_t last_stream = nullptr;
     long long ws_bytes = 0;
@@ -123,6 +124,8 @@ LaunchArgs base_args(necg_handle *h, int K) {
     a.ntiles = h->ntiles;
     a.LC_e = h->lc_e;
     a.LC_g = h->lc_g;
+    a.minb_e = h->minb_e;
+    a.minb_g = h->minb_g;
     a.rows = h->d_rows;
     a.scal = h->d_scal;
     a.part = h->d_part;
@@ -175,7 +178,6 @@ int necg_create(int n, int nst, int K_max, double efs, const double *mass_host,
     // default tile widths per particle count
     h->lc_e = n >= 5 ? 4 : 8;
     h->lc_g = n >= 5 ? 4 : 8;
-    h->lc_g_alloc = 1;  // partial buffer sized for the narrowest gradient tile
     cudaGetDevice(&h->device);
     const size_t K = (size_t)K_max;
     const size_t blk = (size_t)(n * (n + 1) / 2 + 3 * n);
@@ -222,6 +224,13 @@ int necg_set_tiles(necg_handle *h, int lc_energy, int lc_grad) {
         return NECG_ERR_ARG;
     h->lc_e = lc_energy;
     h->lc_g = lc_grad;
+    return NECG_OK;
+}
+
+int necg_set_variant(necg_handle *h, int minb_energy, int minb_grad) {
+    if (!h || minb_energy < 1 || minb_energy > 4 || minb_grad < 1 || minb_grad > 4) return NECG_ERR_ARG;
+    h->minb_e = minb_energy;
+    h->minb_g = minb_grad;
     return NECG_OK;
 }
 

@@ -56,8 +56,8 @@ __global__ void __launch_bounds__(128) prep_ket_kernel(const double *__restrict_
 
 // Energy tiles over the lower triangle (the loop of python/outprod.py:49-54 and
 // python/necg.py:43-50); tile list built by the host (energy_tile_count order).
-template <int N>
-__global__ void __launch_bounds__(128) energy_kernel(const int2 *__restrict__ tiles, int ntiles,
+template <int N, int MINB>
+__global__ void __launch_bounds__(128, MINB) energy_kernel(const int2 *__restrict__ tiles, int ntiles,
                                                      int LC, int K, int nst, Consts<N> cs,
                                                      const double *__restrict__ bra,
                                                      const double *__restrict__ ket,
@@ -162,8 +162,8 @@ __global__ void __launch_bounds__(1024) finalize_kernel(const double *__restrict
 // python/make_grad.py:37-55, contracted with C on the fly as lines 61-79 do).
 // Tile t = (kb, lc); lane k accumulates over l in the chunk and all P and
 // writes its partial to part[(lc * Part::size + f) * K + k].
-template <int N>
-__global__ void __launch_bounds__(128) grad_kernel(int nkb, int nlc, int LC, int K, int nst,
+template <int N, int MINB>
+__global__ void __launch_bounds__(128, MINB) grad_kernel(int nkb, int nlc, int LC, int K, int nst,
                                                    Consts<N> cs, const double *__restrict__ bra,
                                                    const double *__restrict__ ket,
                                                    const double *__restrict__ scal, double lam,
@@ -178,18 +178,30 @@ __global__ void __launch_bounds__(128) grad_kernel(int nkb, int nlc, int LC, int
     if (!ok) flag_status(status, 1, k * K + l0);
 }
 
-// Sum the partials of basis k, scale by norm C_k (python/make_grad.py:61-79)
+// Sum the gradient-tile partials over the ket chunks, in place into chunk 0:
+// one thread per (field, k), coalesced along k.
+__global__ void __launch_bounds__(256) grad_sum_kernel(double *__restrict__ part, int nlc, int K,
+                                                       int PS) {
+    const size_t id = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= (size_t)PS * K) return;
+    double s = part[id];
+    const size_t stride = (size_t)PS * K;
+    for (int lc = 1; lc < nlc; ++lc) s += part[id + lc * stride];
+    part[id] = s;
+}
+
+// Scale the summed partial of basis k by norm C_k (python/make_grad.py:61-79)
 // and write GRADA block k in the reference's parameter order.
 template <int N>
-__global__ void __launch_bounds__(128) grad_reduce_kernel(const double *__restrict__ part, int nlc,
-                                                          int K, const double *__restrict__ bra,
+__global__ void __launch_bounds__(128) grad_reduce_kernel(const double *__restrict__ part, int K,
+                                                          const double *__restrict__ bra,
                                                           const double *__restrict__ C,
                                                           const double *__restrict__ scal,
                                                           double *__restrict__ g, int *status) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= K) return;
     const double sc = scal[1] * (C ? C[k] : 1.0);
-    if (!grad_reduce_one<N>(part, nlc, K, bra, sc, g, k)) atomicOr(status, 2);
+    if (!grad_reduce_one<N>(part, 1, K, bra, sc, g, k)) atomicOr(status, 2);
 }
 
 // Per-term elements for the matel / gradel API: terms[3 t .. 3 t + 2] =
@@ -291,23 +303,42 @@ template <int N> struct Launch {
         prep_ket_kernel<N><<<(nk + 127) / 128, 128, 0, st>>>(a.iv, a.C, a.K, a.nst, cs, a.sml, a.sms,
                                                              a.scvv, a.ket);
     }
-    static void energy(const LaunchArgs &a, cudaStream_t st) {
+    template <int MINB> static void energy_v(const LaunchArgs &a, cudaStream_t st) {
         Consts<N> cs = make_consts<N>(a.mass_h, a.ncv_h, a.efs);
         const int threads = 128, wpb = threads / 32;
-        energy_kernel<N><<<(a.ntiles + wpb - 1) / wpb, threads, 0, st>>>(
+        energy_kernel<N, MINB><<<(a.ntiles + wpb - 1) / wpb, threads, 0, st>>>(
             a.tiles, a.ntiles, a.LC_e, a.K, a.nst, cs, a.bra, a.ket, a.H, a.S, a.Kin, a.Pot, a.status);
     }
-    static void grad_tiles(const LaunchArgs &a, cudaStream_t st) {
+    static void energy(const LaunchArgs &a, cudaStream_t st) {
+        switch (a.minb_e) {
+        case 2: energy_v<2>(a, st); break;
+        case 3: energy_v<3>(a, st); break;
+        case 4: energy_v<4>(a, st); break;
+        default: energy_v<1>(a, st); break;
+        }
+    }
+    template <int MINB> static void grad_v(const LaunchArgs &a, cudaStream_t st) {
         Consts<N> cs = make_consts<N>(a.mass_h, a.ncv_h, a.efs);
         const int nkb = (a.K + 31) / 32, nlc = (a.K + a.LC_g - 1) / a.LC_g;
         const int threads = 128, wpb = threads / 32;
-        grad_kernel<N><<<(nkb * nlc + wpb - 1) / wpb, threads, 0, st>>>(
+        grad_kernel<N, MINB><<<(nkb * nlc + wpb - 1) / wpb, threads, 0, st>>>(
             nkb, nlc, a.LC_g, a.K, a.nst, cs, a.bra, a.ket, a.scal, a.lam, a.part, a.status);
+    }
+    static void grad_tiles(const LaunchArgs &a, cudaStream_t st) {
+        switch (a.minb_g) {
+        case 2: grad_v<2>(a, st); break;
+        case 3: grad_v<3>(a, st); break;
+        case 4: grad_v<4>(a, st); break;
+        default: grad_v<1>(a, st); break;
+        }
     }
     static void grad_reduce(const LaunchArgs &a, cudaStream_t st) {
         const int nlc = (a.K + a.LC_g - 1) / a.LC_g;
-        grad_reduce_kernel<N><<<(a.K + 127) / 128, 128, 0, st>>>(a.part, nlc, a.K, a.bra, a.C, a.scal,
-                                                                  a.g, a.status);
+        constexpr int PS = Part<N>::size;
+        const size_t nthr = (size_t)PS * a.K;
+        if (nlc > 1) grad_sum_kernel<<<(unsigned)((nthr + 255) / 256), 256, 0, st>>>(a.part, nlc, a.K, PS);
+        grad_reduce_kernel<N><<<(a.K + 127) / 128, 128, 0, st>>>(a.part, a.K, a.bra, a.C, a.scal, a.g,
+                                                                  a.status);
     }
     static void matel(const LaunchArgs &a, const int *terms, int nterms, double *out,
                       cudaStream_t st) {

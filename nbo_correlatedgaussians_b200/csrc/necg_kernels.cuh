@@ -13,6 +13,7 @@ struct LaunchArgs {
     double *bra, *ket;                     // device workspace: bra SoA, ket records
     const int2 *tiles;                     // energy tile list (kb, lc)
     int ntiles, LC_e, LC_g;
+    int minb_e, minb_g;                    // kernel variants: min resident blocks per SM
     double *H, *S, *Kin, *Pot;             // device outputs (Kin/Pot optional)
     double *rows, *scal, *part, *g;        // device workspace / outputs
     double lam, scale_override;

@@ -141,7 +141,10 @@ def test_drop_in_modules(torch_cuda, tmp_path):
         assert elem_rel(np.array(matel(*t))[None], ref[None], efs=sh.efs).max() < TOL_ELEM
         tg, tgs = gradel(*t)
         rg, rgs = o.gradel(sh.iv, *t)
-        assert normwise(tg, rg) < 1e-12 and normwise(tgs, rgs) < 1e-12
+        # the bra gradient of the identity self-overlap is analytically zero, so
+        # both sides are rounding noise there: floor the scale at the overlap
+        scale = max(np.abs(rgs).max(), abs(ref[0]))
+        assert normwise(tg, rg) < 1e-12 and np.abs(tgs - rgs).max() < 1e-12 * scale
     assert abs(f0(0.5) - o.f0(0.5)) < 1e-15 and abs(df0(20.0) - o.df0(20.0)) < 1e-15
     del e
 
