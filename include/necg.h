@@ -63,10 +63,11 @@ long long necg_workspace_bytes(const necg_handle *h);
  * defaults are chosen per n. */
 int necg_set_tiles(necg_handle *h, int lc_energy, int lc_grad);
 
-/* Register-budget variant of the energy and gradient tile kernels: the
- * minimum number of resident 128-thread blocks per SM the kernel is compiled
- * for (1..4; more blocks = fewer registers per thread).  Set by the autotuner. */
-int necg_set_variant(necg_handle *h, int minb_energy, int minb_grad);
+/* Register-budget variant of the energy and gradient tile kernels (one warp
+ * per block): the minimum number of resident warps per SM the kernel is
+ * compiled for, one of 8, 12, 16, 20 (2, 3, 4, 5 warps per scheduler: up to
+ * 255, 168, 128, 96 registers per thread).  Set by the autotuner. */
+int necg_set_variant(necg_handle *h, int minw_energy, int minw_grad);
 
 /* One objective evaluation: python/outprod.py:20-76 outprod(x) -> (f, g),
  * including make_grad (python/make_grad.py:18-90).  Device pointers; H_dev and
@@ -82,11 +83,12 @@ int necg_outprod_host(necg_handle *h, int K, const double *x_host, double *f_hos
                       double *g_host, void *stream);
 
 /* Energy only: H, S (and optionally the kinetic and Coulomb parts Kin, Pot,
- * NULL to skip) and f = C^T H C / C^T S C when C_dev and f_dev are non-NULL.
+ * NULL to skip); when C_dev and en_dev are non-NULL, en_dev[0..1] receive
+ * E = C^T H C / C^T S C and norm = 1 / C^T S C.
  * python/necg.py:36-58 (_build_matrices) and python/outprod.py:46-68. */
 int necg_build_matrices(necg_handle *h, int K, const double *iv_dev, const double *C_dev,
                         double *H_dev, double *S_dev, double *Kin_dev, double *Pot_dev,
-                        double *f_dev, void *stream);
+                        double *en_dev, void *stream);
 
 /* python/make_grad.py:18-90 make_grad(eng, norm): gradient of the Rayleigh
  * quotient for given energy and normalisation, with GRADC from the supplied
@@ -94,6 +96,13 @@ int necg_build_matrices(necg_handle *h, int K, const double *iv_dev, const doubl
 int necg_make_grad(necg_handle *h, int K, const double *iv_dev, const double *C_dev,
                    const double *H_dev, const double *S_dev, double eng, double norm,
                    double *g_dev, void *stream);
+
+/* necg_make_grad with E and norm read from device memory (en_dev[0..1], as
+ * written by necg_build_matrices): no host round trip, so a forward energy and
+ * this backward gradient can be enqueued back to back or captured in a graph. */
+int necg_make_grad_dev(necg_handle *h, int K, const double *iv_dev, const double *C_dev,
+                       const double *H_dev, const double *S_dev, const double *en_dev,
+                       double *g_dev, void *stream);
 
 /* python/matel.py:28-210 matel(stf, ii, jj) for a batch of terms.
  * terms_dev: nterms * 3 ints (stf, ii, jj), 1-based.  out_dev: nterms * 4
@@ -109,6 +118,43 @@ int necg_gradel(necg_handle *h, int K, const double *iv_dev, int nterms, const i
 
 /* python/utils.py:78-106 f0(z) and df0(z) on an array (either output may be NULL). */
 int necg_f0(const double *z_dev, int count, double *f_dev, double *df_dev, void *stream);
+
+/* ---- batched evaluation -------------------------------------------------
+ * Many independent instances (handles of any n, nst, K) evaluated in one step:
+ * every per-pair phase is one persistent launch over a flattened queue of
+ * (instance, tile) work items ordered by decreasing cost; the step is a fixed
+ * sequence of eight kernels with fixed grids, so it can be captured once in a
+ * CUDA graph and replayed for any plan.  No counterpart in the reference, which
+ * evaluates one basis per process (python/outprod.py:20). */
+typedef struct necg_batch necg_batch;
+
+/* Capacity: instances per plan and tiles per queue. */
+int necg_batch_create(int max_instances, int max_tiles, necg_batch **out);
+int necg_batch_destroy(necg_batch *b);
+
+/* Set the instances of the next step: for instance q, handle hs[q] with basis
+ * size Ks[q] (<= its K_max), input x_dev[q] = [iv, C] and outputs g_dev[q]
+ * (gradient) and f_dev[q] (energy; f_dev may be NULL).  Each handle's own tile
+ * widths are used.  Uploads the plan on `stream`; the device plan buffer is
+ * overwritten in stream order, so a step already enqueued on `stream` keeps
+ * the plan it was launched with.  Two necg_batch objects used alternately let
+ * the host plan one step while the previous one runs. */
+int necg_batch_plan(necg_batch *b, int count, necg_handle *const *hs, const int *Ks,
+                    const double *const *x_dev, double *const *g_dev, double *const *f_dev,
+                    void *stream);
+
+/* Launch one step of the current plan. */
+int necg_batch_step(necg_batch *b, void *stream);
+
+/* Capture the step into a CUDA graph (once; the graph reads the plan from
+ * device memory, so it stays valid across necg_batch_plan calls with the same
+ * capacity) and replay it. */
+int necg_batch_graph(necg_batch *b, void *stream);
+int necg_batch_replay(necg_batch *b, void *stream);
+
+/* Per-instance status of the last step (synchronises `stream`); returns the
+ * first non-OK code or NECG_OK. */
+int necg_batch_status(necg_batch *b, int *status_out, void *stream);
 
 /* Synchronise the handle's last stream and report the pair status of the most
  * recent evaluation: NECG_OK, NECG_ERR_NOT_PD or NECG_ERR_NONFINITE; *bad_pair

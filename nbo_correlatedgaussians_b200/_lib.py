@@ -36,10 +36,18 @@ SIGNATURES = [
     ("necg_outprod_host", _i, [_vp, _i, _vp, _vp, _vp, _vp]),
     ("necg_build_matrices", _i, [_vp, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     ("necg_make_grad", _i, [_vp, _i, _vp, _vp, _vp, _vp, _d, _d, _vp, _vp]),
+    ("necg_make_grad_dev", _i, [_vp, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     ("necg_matel", _i, [_vp, _i, _vp, _i, _vp, _vp, _vp]),
     ("necg_gradel", _i, [_vp, _i, _vp, _i, _vp, _vp, _vp, _vp]),
     ("necg_f0", _i, [_vp, _i, _vp, _vp, _vp]),
     ("necg_status", _i, [_vp, ctypes.POINTER(_ll)]),
+    ("necg_batch_create", _i, [_i, _i, ctypes.POINTER(_vp)]),
+    ("necg_batch_destroy", _i, [_vp]),
+    ("necg_batch_plan", _i, [_vp, _i, _vp, _vp, _vp, _vp, _vp, _vp]),
+    ("necg_batch_step", _i, [_vp, _vp]),
+    ("necg_batch_graph", _i, [_vp, _vp]),
+    ("necg_batch_replay", _i, [_vp, _vp]),
+    ("necg_batch_status", _i, [_vp, _vp, _vp]),
     ("necg_status_string", ctypes.c_char_p, [_i]),
     ("necg_profile", _i, [_vp, _i]),
     ("necg_fp64_peak", _i, [_i, _dp, _vp]),

@@ -9,8 +9,10 @@ bucket (powers of two), so a run pays for tuning once.
 The search space:
   LC_e   ket chunk of an energy tile (kets per warp per tile)
   LC_g   ket chunk of a gradient tile (also sets the partial-buffer depth)
-  minb   minimum resident 128-thread blocks per SM the kernel is compiled for
-         (1: up to 255 registers per thread; 3: 168; 4: 128)
+  minw   minimum resident warps per SM the kernel is compiled for (one warp
+         per block): 8 -> up to 255 registers per thread, 12 -> 168, 16 -> 128,
+         20 -> 96 (the register file is split between the four schedulers, so
+         these are the only distinct budgets)
 """
 from __future__ import annotations
 
@@ -28,7 +30,7 @@ CACHE = os.environ.get("NECG_TUNE_CACHE", os.path.join(os.path.dirname(os.path.a
 
 LC_E = (2, 4, 8, 16, 32)
 LC_G = (4, 8, 16, 32, 64)
-MINB = (1, 3, 4)
+MINB = (8, 12, 16, 20)
 
 
 def _bucket(K: int) -> int:

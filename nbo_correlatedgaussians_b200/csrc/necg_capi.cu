@@ -18,31 +18,11 @@
 
 #include <vector>
 
+#include "necg_handle.h"
 #include "necg_kernels.cuh"
 #include "necg_math.cuh"
-#include "../../include/necg.h"
 
 using necg::LaunchArgs;
-
-struct necg_handle {
-    int n, nst, K_max;
-    double efs;
-    std::vector<double> mass, ncv, scvv, sml, sms;
-    double *d_sml = nullptr, *d_sms = nullptr, *d_scvv = nullptr;
-    double *d_bra = nullptr, *d_ket = nullptr, *d_part = nullptr;
-    double *d_H = nullptr, *d_S = nullptr, *d_rows = nullptr, *d_scal = nullptr;
-    double *d_x = nullptr, *d_g = nullptr, *d_f = nullptr;
-    int *d_status = nullptr;
-    int2 *d_tiles = nullptr;
-    int tiles_cap = 0, tiles_K = -1, tiles_lc = -1, ntiles = 0;
-    int lc_e = 8, lc_g = 8;
-    int minb_e = 1, minb_g = 1;
-    int device = 0;
-    cudaStream_t last_stream = nullptr;
-    long long ws_bytes = 0;
-    bool profile = false;
-    cudaEvent_t ev[6] = {};
-};
 
 namespace {
 
@@ -227,16 +207,17 @@ int necg_set_tiles(necg_handle *h, int lc_energy, int lc_grad) {
     return NECG_OK;
 }
 
-int necg_set_variant(necg_handle *h, int minb_energy, int minb_grad) {
-    if (!h || minb_energy < 1 || minb_energy > 4 || minb_grad < 1 || minb_grad > 4) return NECG_ERR_ARG;
-    h->minb_e = minb_energy;
-    h->minb_g = minb_grad;
+int necg_set_variant(necg_handle *h, int minw_energy, int minw_grad) {
+    auto okw = [](int w) { return w == 8 || w == 12 || w == 16 || w == 20; };
+    if (!h || !okw(minw_energy) || !okw(minw_grad)) return NECG_ERR_ARG;
+    h->minb_e = minw_energy;
+    h->minb_g = minw_grad;
     return NECG_OK;
 }
 
 int necg_build_matrices(necg_handle *h, int K, const double *iv_dev, const double *C_dev,
                         double *H_dev, double *S_dev, double *Kin_dev, double *Pot_dev,
-                        double *f_dev, void *stream) {
+                        double *en_dev, void *stream) {
     int rc = check_K(h, K);
     if (rc) return rc;
     if (!iv_dev) return NECG_ERR_ARG;
@@ -252,7 +233,7 @@ int necg_build_matrices(necg_handle *h, int K, const double *iv_dev, const doubl
     a.Pot = Pot_dev;
     if (necg::launch_prep(a, st)) return NECG_ERR_UNSUPPORTED;
     necg::launch_energy(a, st);
-    if (C_dev && f_dev) necg::launch_rows_finalize(a, f_dev, nullptr, 0, 0.0, 0.0, st);
+    if (C_dev && en_dev) necg::launch_rows_finalize(a, nullptr, nullptr, 0, 0.0, 0.0, st, nullptr, en_dev);
     return finish_launch();
 }
 
@@ -320,6 +301,27 @@ int necg_make_grad(necg_handle *h, int K, const double *iv_dev, const double *C_
     // GRADC = 2 norm (H - eng S) C with the caller's eng and norm; also sets
     // the E and norm the gradient tiles read
     necg::launch_rows_finalize(a, nullptr, g_dev + siv, 1, eng, norm, st);
+    necg::launch_grad(a, st);
+    return finish_launch();
+}
+
+int necg_make_grad_dev(necg_handle *h, int K, const double *iv_dev, const double *C_dev,
+                       const double *H_dev, const double *S_dev, const double *en_dev, double *g_dev,
+                       void *stream) {
+    int rc = check_K(h, K);
+    if (rc) return rc;
+    if (!iv_dev || !C_dev || !H_dev || !S_dev || !en_dev || !g_dev) return NECG_ERR_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    if ((rc = begin(h, st))) return rc;
+    const size_t siv = (size_t)K * (h->n * (h->n + 1) / 2 + 3 * h->n);
+    LaunchArgs a = base_args(h, K);
+    a.iv = iv_dev;
+    a.C = C_dev;
+    a.H = const_cast<double *>(H_dev);
+    a.S = const_cast<double *>(S_dev);
+    a.g = g_dev;
+    if (necg::launch_prep(a, st)) return NECG_ERR_UNSUPPORTED;
+    necg::launch_rows_finalize(a, nullptr, g_dev + siv, 2, 0.0, 0.0, st, en_dev, nullptr);
     necg::launch_grad(a, st);
     return finish_launch();
 }

@@ -1,0 +1,28 @@
+// necg_handle.h -- internal layout of the opaque necg_handle (one particle
+// system + symmetry set + device workspace for bases of up to K_max functions).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "../../include/necg.h"
+
+struct necg_handle {
+    int n, nst, K_max;
+    double efs;
+    std::vector<double> mass, ncv, scvv, sml, sms;
+    double *d_sml = nullptr, *d_sms = nullptr, *d_scvv = nullptr;
+    double *d_bra = nullptr, *d_ket = nullptr, *d_part = nullptr;
+    double *d_H = nullptr, *d_S = nullptr, *d_rows = nullptr, *d_scal = nullptr;
+    double *d_x = nullptr, *d_g = nullptr, *d_f = nullptr;
+    int *d_status = nullptr;
+    int2 *d_tiles = nullptr;
+    int tiles_cap = 0, tiles_K = -1, tiles_lc = -1, ntiles = 0;
+    int lc_e = 8, lc_g = 8;
+    int minb_e = 16, minb_g = 8;
+    int device = 0;
+    cudaStream_t last_stream = nullptr;
+    long long ws_bytes = 0;
+    bool profile = false;
+    cudaEvent_t ev[6] = {};
+};

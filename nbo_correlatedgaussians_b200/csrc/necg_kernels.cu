@@ -56,8 +56,10 @@ __global__ void __launch_bounds__(128) prep_ket_kernel(const double *__restrict_
 
 // Energy tiles over the lower triangle (the loop of python/outprod.py:49-54 and
 // python/necg.py:43-50); tile list built by the host (energy_tile_count order).
-template <int N, int MINB>
-__global__ void __launch_bounds__(128, MINB) energy_kernel(const int2 *__restrict__ tiles, int ntiles,
+// One warp per block; MINW = minimum resident warps per SM the kernel is
+// compiled for (register budget 65536 / (32 MINW) per thread).
+template <int N, int MINW>
+__global__ void __launch_bounds__(32, MINW) energy_kernel(const int2 *__restrict__ tiles, int ntiles,
                                                      int LC, int K, int nst, Consts<N> cs,
                                                      const double *__restrict__ bra,
                                                      const double *__restrict__ ket,
@@ -112,7 +114,9 @@ __global__ void __launch_bounds__(1024) finalize_kernel(const double *__restrict
                                                         double *__restrict__ scal,
                                                         double *__restrict__ f_out,
                                                         double *__restrict__ gradc, int *status,
-                                                        int given, double eng, double gnorm) {
+                                                        int given, double eng, double gnorm,
+                                                        const double *__restrict__ given_dev,
+                                                        double *__restrict__ en_out) {
     __shared__ double sh[2][32];
     double ah = 0.0, as = 0.0;
     for (int i = threadIdx.x; i < K; i += blockDim.x) {
@@ -140,13 +144,23 @@ __global__ void __launch_bounds__(1024) finalize_kernel(const double *__restrict
             as += __shfl_xor_sync(0xffffffffu, as, o);
         }
         if (lane == 0) {
-            const double E = given ? eng : ah / as;
-            const double nrm = given ? gnorm : 1.0 / as;
+            double E = ah / as, nrm = 1.0 / as;
+            if (given == 1) {
+                E = eng;
+                nrm = gnorm;
+            } else if (given == 2) {
+                E = given_dev[0];
+                nrm = given_dev[1];
+            }
             scal[0] = E;
             scal[1] = nrm;
             scal[2] = ah;
             scal[3] = as;
             if (f_out) *f_out = E;
+            if (en_out) {
+                en_out[0] = E;
+                en_out[1] = nrm;
+            }
             if (!isfinite(E)) atomicOr(status, 2);
         }
     }
@@ -162,8 +176,8 @@ __global__ void __launch_bounds__(1024) finalize_kernel(const double *__restrict
 // python/make_grad.py:37-55, contracted with C on the fly as lines 61-79 do).
 // Tile t = (kb, lc); lane k accumulates over l in the chunk and all P and
 // writes its partial to part[(lc * Part::size + f) * K + k].
-template <int N, int MINB>
-__global__ void __launch_bounds__(128, MINB) grad_kernel(int nkb, int nlc, int LC, int K, int nst,
+template <int N, int MINW>
+__global__ void __launch_bounds__(32, MINW) grad_kernel(int nkb, int nlc, int LC, int K, int nst,
                                                    Consts<N> cs, const double *__restrict__ bra,
                                                    const double *__restrict__ ket,
                                                    const double *__restrict__ scal, double lam,
@@ -303,33 +317,31 @@ template <int N> struct Launch {
         prep_ket_kernel<N><<<(nk + 127) / 128, 128, 0, st>>>(a.iv, a.C, a.K, a.nst, cs, a.sml, a.sms,
                                                              a.scvv, a.ket);
     }
-    template <int MINB> static void energy_v(const LaunchArgs &a, cudaStream_t st) {
+    template <int MINW> static void energy_v(const LaunchArgs &a, cudaStream_t st) {
         Consts<N> cs = make_consts<N>(a.mass_h, a.ncv_h, a.efs);
-        const int threads = 128, wpb = threads / 32;
-        energy_kernel<N, MINB><<<(a.ntiles + wpb - 1) / wpb, threads, 0, st>>>(
-            a.tiles, a.ntiles, a.LC_e, a.K, a.nst, cs, a.bra, a.ket, a.H, a.S, a.Kin, a.Pot, a.status);
+        energy_kernel<N, MINW><<<a.ntiles, 32, 0, st>>>(a.tiles, a.ntiles, a.LC_e, a.K, a.nst, cs, a.bra,
+                                                        a.ket, a.H, a.S, a.Kin, a.Pot, a.status);
     }
     static void energy(const LaunchArgs &a, cudaStream_t st) {
         switch (a.minb_e) {
-        case 2: energy_v<2>(a, st); break;
-        case 3: energy_v<3>(a, st); break;
-        case 4: energy_v<4>(a, st); break;
-        default: energy_v<1>(a, st); break;
+        case 12: energy_v<12>(a, st); break;
+        case 16: energy_v<16>(a, st); break;
+        case 20: energy_v<20>(a, st); break;
+        default: energy_v<8>(a, st); break;
         }
     }
-    template <int MINB> static void grad_v(const LaunchArgs &a, cudaStream_t st) {
+    template <int MINW> static void grad_v(const LaunchArgs &a, cudaStream_t st) {
         Consts<N> cs = make_consts<N>(a.mass_h, a.ncv_h, a.efs);
         const int nkb = (a.K + 31) / 32, nlc = (a.K + a.LC_g - 1) / a.LC_g;
-        const int threads = 128, wpb = threads / 32;
-        grad_kernel<N, MINB><<<(nkb * nlc + wpb - 1) / wpb, threads, 0, st>>>(
-            nkb, nlc, a.LC_g, a.K, a.nst, cs, a.bra, a.ket, a.scal, a.lam, a.part, a.status);
+        grad_kernel<N, MINW><<<nkb * nlc, 32, 0, st>>>(nkb, nlc, a.LC_g, a.K, a.nst, cs, a.bra, a.ket,
+                                                       a.scal, a.lam, a.part, a.status);
     }
     static void grad_tiles(const LaunchArgs &a, cudaStream_t st) {
         switch (a.minb_g) {
-        case 2: grad_v<2>(a, st); break;
-        case 3: grad_v<3>(a, st); break;
-        case 4: grad_v<4>(a, st); break;
-        default: grad_v<1>(a, st); break;
+        case 12: grad_v<12>(a, st); break;
+        case 16: grad_v<16>(a, st); break;
+        case 20: grad_v<20>(a, st); break;
+        default: grad_v<8>(a, st); break;
         }
     }
     static void grad_reduce(const LaunchArgs &a, cudaStream_t st) {
@@ -395,10 +407,10 @@ int launch_gradel(const LaunchArgs &a, const int *terms, int nterms, double *tg,
     return 0;
 }
 void launch_rows_finalize(const LaunchArgs &a, double *f_out, double *gradc, int given, double eng,
-                          double norm, cudaStream_t st) {
+                          double norm, cudaStream_t st, const double *given_dev, double *en_out) {
     rows_kernel<<<(a.K * 32 + 255) / 256, 256, 0, st>>>(a.H, a.S, a.C, a.K, a.rows);
     finalize_kernel<<<1, 1024, 0, st>>>(a.rows, a.C, a.K, a.scal, f_out, gradc, a.status, given, eng,
-                                        norm);
+                                        norm, given_dev, en_out);
 }
 void launch_reset_status(int *status, cudaStream_t st) { reset_status_kernel<<<1, 1, 0, st>>>(status); }
 void launch_fp64_probe(int blocks, int iters, double *sink, cudaStream_t st) {

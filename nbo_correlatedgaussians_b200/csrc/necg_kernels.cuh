@@ -28,8 +28,11 @@ int launch_grad_reduce(const LaunchArgs &a, cudaStream_t st);
 int launch_matel(const LaunchArgs &a, const int *terms, int nterms, double *out, cudaStream_t st);
 int launch_gradel(const LaunchArgs &a, const int *terms, int nterms, double *tg, double *tgs,
                   cudaStream_t st);
+// given: 0 compute E and norm from C, H, S; 1 use (eng, norm); 2 read them
+// from given_dev[0..1].  en_out (optional) receives {E, norm}.
 void launch_rows_finalize(const LaunchArgs &a, double *f_out, double *gradc, int given,
-                          double eng, double norm, cudaStream_t st);
+                          double eng, double norm, cudaStream_t st,
+                          const double *given_dev = nullptr, double *en_out = nullptr);
 void launch_reset_status(int *status, cudaStream_t st);
 void launch_fp64_probe(int blocks, int iters, double *sink, cudaStream_t st);
 void launch_f0(const double *z, int count, double *f, double *df, cudaStream_t st);

@@ -138,9 +138,11 @@ class Engine:
         return f.value, g
 
     # ------------------------------------------------------- matrix build
-    def build_matrices(self, iv, C=None, K: int | None = None, parts: bool = True, stream=None):
+    def build_matrices(self, iv, C=None, K: int | None = None, parts: bool = True, stream=None,
+                       check: bool = True):
         """H, S (and Kinetic, Potential when ``parts``) as device tensors; also
-        f = C^T H C / C^T S C when C is given (python/necg.py:36-71)."""
+        en = [E, norm] with E = C^T H C / C^T S C, norm = 1 / C^T S C when C is
+        given (python/necg.py:36-71)."""
         iv = self._tensor(iv)
         K = K or iv.numel() // self.blk
         dev = self.device
@@ -149,12 +151,13 @@ class Engine:
         Kin = torch.empty_like(H) if parts else None
         Pot = torch.empty_like(H) if parts else None
         Ct = self._tensor(C) if C is not None else None
-        f = torch.empty(1, dtype=torch.float64, device=dev) if C is not None else None
+        en = torch.empty(2, dtype=torch.float64, device=dev) if C is not None else None
         rc = self.L.necg_build_matrices(self.h, K, iv.data_ptr(), _ptr(Ct), H.data_ptr(), S.data_ptr(),
-                                        _ptr(Kin), _ptr(Pot), _ptr(f), _stream_ptr(stream))
+                                        _ptr(Kin), _ptr(Pot), _ptr(en), _stream_ptr(stream))
         _lib.check(rc, "necg_build_matrices")
-        self.raise_status("build_matrices")
-        return H, S, Kin, Pot, f
+        if check:
+            self.raise_status("build_matrices")
+        return H, S, Kin, Pot, en
 
     def make_grad(self, iv, C, H, S, eng: float, norm: float, stream=None) -> torch.Tensor:
         iv, C, H, S = (self._tensor(a) for a in (iv, C, H, S))
@@ -164,6 +167,16 @@ class Engine:
                                    float(eng), float(norm), g.data_ptr(), _stream_ptr(stream))
         _lib.check(rc, "necg_make_grad")
         self.raise_status("make_grad")
+        return g
+
+    def make_grad_dev(self, iv, C, H, S, en, stream=None) -> torch.Tensor:
+        """Gradient with E and norm read from the device tensor en = [E, norm]."""
+        iv, C, H, S, en = (self._tensor(a) for a in (iv, C, H, S, en))
+        K = C.numel()
+        g = torch.empty(self._len(K), dtype=torch.float64, device=self.device)
+        rc = self.L.necg_make_grad_dev(self.h, K, iv.data_ptr(), C.data_ptr(), H.data_ptr(), S.data_ptr(),
+                                       en.data_ptr(), g.data_ptr(), _stream_ptr(stream))
+        _lib.check(rc, "necg_make_grad_dev")
         return g
 
     # ------------------------------------------------------ single terms

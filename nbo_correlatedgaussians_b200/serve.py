@@ -1,0 +1,266 @@
+"""Serving loop for many concurrent optimiser runs (continuous batching).
+
+Each run is one basis being optimised by its own client (e.g. a truncated-Newton
+minimiser calling ``evaluate(x)`` as its objective, the role outprod plays for
+the reference's optimiser, python/necg.py:159-171 and source/tn.f).  The server:
+
+* keeps each admitted run's state on the device: its ``Engine`` (bra/ket
+  records, H, S, gradient partials for its K), its parameters x = [iv, C] and
+  its outputs g, E;
+* admits runs under an HBM budget and a slot count: a run that does not fit
+  waits until earlier runs close and free their workspace;
+* batches continuously: a worker thread takes every request that is ready,
+  plans one batched step over those runs (all their energy and gradient tiles
+  in two flattened queues) and launches it as a CUDA-graph replay.  Requests
+  that arrive while a step is on the GPU go into the next step; two batch
+  plans are used alternately, so the host plans step i+1 while step i runs.
+* reports per-request latency (submit to result) and throughput.
+
+Because every run's tiles and reductions are the same in any batch, a run's
+results do not depend on which other runs share its steps.
+"""
+from __future__ import annotations
+
+import collections
+import threading
+import time
+
+import numpy as np
+import torch
+
+from . import _lib
+from .autotune import tuned
+from .batch import Batch
+from .engine import Engine
+from .problem import Problem
+
+
+def workspace_estimate(p: Problem, K_max: int | None = None) -> int:
+    """Device bytes a run's Engine allocates (mirror of necg_create's sizes)."""
+    K, n, nst = int(K_max or p.K), p.n, p.nst
+    tri = n * (n + 1) // 2
+    ket = (tri + 6 * n + tri + n * n + 5 + 1) & ~1
+    bra = tri + 6 * n + tri + 3 + tri
+    ps = tri + 1 + 3 * n
+    blk = tri + 3 * n
+    doubles = (bra * K + ket * K * nst + ps * K * ((K + 3) // 4) + 2 * K * K + 2 * K + 4
+               + 2 * (K * blk + K) + 2 + nst * (n * n + 9 * n * n + 1))
+    return 8 * doubles + 3 * 8 * (K * blk + K) + 4096
+
+
+class Run:
+    def __init__(self, rid: int, problem: Problem):
+        self.id = rid
+        self.problem = problem
+        self.engine: Engine | None = None
+        self.bytes = workspace_estimate(problem)
+        self.x = self.g = self.f = None
+        self.xh = self.gh = self.fh = None
+        self.admitted = threading.Event()
+        self.evals = 0
+        self.closed = False
+
+
+class Request:
+    __slots__ = ("run", "x", "done", "f", "g", "t_submit", "t_done", "error")
+
+    def __init__(self, run: Run, x: np.ndarray):
+        self.run = run
+        self.x = x
+        self.done = threading.Event()
+        self.f = None
+        self.g = None
+        self.error = None
+        self.t_submit = time.perf_counter()
+        self.t_done = None
+
+
+class Server:
+    def __init__(self, budget_bytes: float = 120e9, max_slots: int = 256, graph: bool = True, tune: bool = True,
+                 device=None):
+        self.budget = float(budget_bytes)
+        self.max_slots = int(max_slots)
+        self.graph = graph
+        self.tune = tune
+        self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        self.lock = threading.Condition()
+        self.pending: collections.deque[Request] = collections.deque()
+        self.waiting_runs: collections.deque[Run] = collections.deque()
+        self.runs: dict[int, Run] = {}
+        self.used = 0
+        self.next_id = 0
+        self.latencies: list[float] = []
+        self.steps = 0
+        self.step_sizes: list[int] = []
+        self._stop = False
+        self._thread = None
+        self.batches = None
+        self.stream = None
+        self.t_start = None
+        self.evals_done = 0
+
+    # ----------------------------------------------------------- lifecycle
+    def start(self) -> "Server":
+        self.stream = torch.cuda.Stream(device=self.device)
+        self.batches = [Batch(self.max_slots), Batch(self.max_slots)]
+        self.t_start = time.perf_counter()
+        self._thread = threading.Thread(target=self._loop, name="necg-server", daemon=True)
+        self._thread.start()
+        return self
+
+    def stop(self) -> None:
+        with self.lock:
+            self._stop = True
+            self.lock.notify_all()
+        if self._thread:
+            self._thread.join()
+        for b in self.batches or []:
+            b.close()
+
+    def __enter__(self):
+        return self.start()
+
+    def __exit__(self, *exc):
+        self.stop()
+
+    # ------------------------------------------------------------- clients
+    def open_run(self, problem: Problem, timeout: float | None = None) -> Run:
+        """Register a run; blocks until it is admitted (memory budget and slots)."""
+        if problem.n > 5:
+            raise ValueError("the batched path supports n <= 5")
+        with self.lock:
+            run = Run(self.next_id, problem)
+            self.next_id += 1
+            if run.bytes > self.budget:
+                raise MemoryError(f"run needs {run.bytes} bytes, more than the whole budget {self.budget:.0f}")
+            self.waiting_runs.append(run)
+            self._admit_locked()
+        if not run.admitted.wait(timeout):
+            raise TimeoutError("run was not admitted in time")
+        return run
+
+    def close_run(self, run: Run) -> None:
+        with self.lock:
+            if run.closed:
+                return
+            run.closed = True
+            self.runs.pop(run.id, None)
+            if run.engine is not None:
+                self.used -= run.bytes
+                # free after in-flight steps that may still reference this run
+                eng = run.engine
+                run.engine = None
+                self.stream.synchronize()
+                eng.close()
+            self._admit_locked()
+
+    def evaluate(self, run: Run, x: np.ndarray, timeout: float | None = None):
+        """E and gradient at x = [iv, C] for this run (blocking)."""
+        if run.engine is None:
+            raise RuntimeError("run is not admitted or already closed")
+        req = Request(run, np.ascontiguousarray(x, dtype=np.float64))
+        with self.lock:
+            self.pending.append(req)
+            self.lock.notify_all()
+        if not req.done.wait(timeout):
+            raise TimeoutError("request timed out")
+        if req.error is not None:
+            raise req.error
+        return req.f, req.g
+
+    def _admit_locked(self) -> None:
+        while self.waiting_runs:
+            run = self.waiting_runs[0]
+            if len(self.runs) >= self.max_slots or self.used + run.bytes > self.budget:
+                return
+            self.waiting_runs.popleft()
+            p = run.problem
+            with torch.cuda.device(self.device):
+                run.engine = Engine(p, device=self.device)
+                run.x = torch.from_numpy(np.ascontiguousarray(p.x)).to(self.device)
+                run.g = torch.empty_like(run.x)
+                run.f = torch.zeros(1, dtype=torch.float64, device=self.device)
+                run.xh = torch.empty(run.x.numel(), dtype=torch.float64).pin_memory()
+                run.gh = torch.empty(run.x.numel(), dtype=torch.float64).pin_memory()
+                run.fh = torch.empty(1, dtype=torch.float64).pin_memory()
+                if self.tune:
+                    tuned(run.engine, run.x, p.K)
+            self.used += run.bytes
+            self.runs[run.id] = run
+            run.admitted.set()
+
+    # -------------------------------------------------------------- worker
+    def _loop(self) -> None:
+        in_flight = None  # (requests, event)
+        wave = 0
+        with torch.cuda.device(self.device):
+            while True:
+                with self.lock:
+                    while not self.pending and in_flight is None and not self._stop:
+                        self.lock.wait()
+                    if self._stop and not self.pending and in_flight is None:
+                        return
+                    # at most one request per run per step (runs issue back to back)
+                    reqs, seen, rest = [], set(), collections.deque()
+                    while self.pending:
+                        r = self.pending.popleft()
+                        if r.run.id in seen:
+                            rest.append(r)
+                        else:
+                            seen.add(r.run.id)
+                            reqs.append(r)
+                    self.pending = rest
+                new_flight = None
+                if reqs:
+                    new_flight = self._launch(reqs, self.batches[wave % 2])
+                    wave += 1
+                if in_flight is not None:
+                    self._deliver(*in_flight)
+                in_flight = new_flight
+
+    def _launch(self, reqs: list[Request], batch: Batch):
+        s = self.stream
+        with torch.cuda.stream(s):
+            for r in reqs:
+                r.run.xh.numpy()[:] = r.x
+                r.run.x.copy_(r.run.xh, non_blocking=True)
+            runs = [r.run for r in reqs]
+            batch.plan([u.engine for u in runs], [u.problem.K for u in runs], [u.x for u in runs],
+                       [u.g for u in runs], [u.f for u in runs], stream=s)
+            batch.step(self.graph, stream=s)
+            for u in runs:
+                u.gh.copy_(u.g, non_blocking=True)
+                u.fh.copy_(u.f, non_blocking=True)
+            ev = torch.cuda.Event()
+            ev.record(s)
+        self.steps += 1
+        self.step_sizes.append(len(reqs))
+        return reqs, ev, batch
+
+    def _deliver(self, reqs: list[Request], ev, batch: Batch) -> None:
+        ev.synchronize()
+        codes = batch.status(stream=self.stream)
+        now = time.perf_counter()
+        for r, code in zip(reqs, codes):
+            if code == _lib.NECG_ERR_NOT_PD:
+                r.error = np.linalg.LinAlgError("A_k + A_l' is not positive definite for some basis pair")
+            elif code != _lib.NECG_OK:
+                r.error = _lib.NecgError(code, f"run {r.run.id}")
+            else:
+                r.f = float(r.run.fh[0])
+                r.g = r.run.gh.numpy().copy()
+            r.t_done = now
+            r.run.evals += 1
+            self.latencies.append(now - r.t_submit)
+            self.evals_done += 1
+            r.done.set()
+
+    # ------------------------------------------------------------ metrics
+    def stats(self) -> dict:
+        lat = np.array(self.latencies) if self.latencies else np.zeros(1)
+        wall = time.perf_counter() - (self.t_start or time.perf_counter())
+        return {"requests": len(self.latencies), "steps": self.steps,
+                "mean_batch": float(np.mean(self.step_sizes)) if self.step_sizes else 0.0,
+                "p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
+                "evals_per_s": self.evals_done / wall if wall > 0 else 0.0, "wall_s": wall,
+                "hbm_used_bytes": self.used}

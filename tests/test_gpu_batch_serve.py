@@ -1,0 +1,184 @@
+"""Autograd Function, batched persistent launch (with CUDA graph replay) and
+the continuous-batching server, on the GPU."""
+import threading
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+from oracle.oracle import Oracle  # noqa: E402
+from _util import TOL_E, TOL_G, normwise  # noqa: E402
+
+
+@pytest.fixture(scope="module")
+def torch_cuda():
+    import torch
+    assert torch.cuda.is_available()
+    return torch
+
+
+def _mixed(seed=0):
+    from nbo_correlatedgaussians_b200 import synth
+    return [synth.make_problem("He", 40, seed + 1), synth.make_problem("H2", 70, seed + 2),
+            synth.make_problem("LiH", 33, seed + 3), synth.make_problem("He", 17, seed + 4),
+            synth.make_problem("H2", 9, seed + 5)]
+
+
+def test_autograd_backward_is_the_gradient_kernel(torch_cuda):
+    torch = torch_cuda
+    from nbo_correlatedgaussians_b200 import synth
+    from nbo_correlatedgaussians_b200.autograd import energy
+    from nbo_correlatedgaussians_b200.engine import Engine
+    p = synth.make_problem("H2", 96, 2)
+    p.C = np.random.default_rng(5).normal(size=p.K)
+    eng = Engine(p)
+    iv = torch.tensor(p.iv, device="cuda", requires_grad=True)
+    C = torch.tensor(p.C, device="cuda", requires_grad=True)
+    E = energy(iv, C, eng)
+    (3.0 * E).backward()
+    fo, go = Oracle.from_problem(p).outprod(p.x, nthreads=8)
+    assert abs(float(E) - fo) < TOL_E
+    g = torch.cat([iv.grad, C.grad]).cpu().numpy()
+    assert normwise(g, 3.0 * go) < TOL_G
+
+
+def test_autograd_central_differences(torch_cuda):
+    """Config 2 check at a reduced size: gradient of the autograd energy against
+    the oracle's gradel-based gradient and against central differences with
+    h = 1e-6 on 64 random parameters (reported; FD noise limits it to ~1e-6)."""
+    torch = torch_cuda
+    from nbo_correlatedgaussians_b200 import synth
+    from nbo_correlatedgaussians_b200.autograd import energy
+    from nbo_correlatedgaussians_b200.engine import Engine
+    p = synth.make_problem("H2", 128, 2)
+    eng = Engine(p)
+    x = torch.tensor(p.x, device="cuda")
+    siv = p.siv
+    xg = x.clone().requires_grad_(True)
+    E = energy(xg[:siv], xg[siv:], eng)
+    E.backward()
+    g = xg.grad.cpu().numpy()
+    _, go = Oracle.from_problem(p).outprod(p.x, nthreads=8)
+    assert normwise(g, go) < TOL_G
+    idx = np.random.default_rng(2).choice(p.x.size, 64, replace=False)
+    h = 1e-6
+    fd = []
+    for i in idx:
+        xp = x.clone()
+        xp[i] += h
+        xm = x.clone()
+        xm[i] -= h
+        ep = float(energy(xp[:siv], xp[siv:], eng))
+        em = float(energy(xm[:siv], xm[siv:], eng))
+        fd.append((ep - em) / (2 * h))
+    fd = np.array(fd)
+    err = np.max(np.abs(fd - g[idx])) / np.max(np.abs(g[idx]))
+    assert err < 1e-4, err
+
+
+def test_batch_matches_single_and_is_order_independent(torch_cuda):
+    from nbo_correlatedgaussians_b200.batch import BatchEngine
+    from nbo_correlatedgaussians_b200.engine import Engine
+    probs = _mixed()
+    be = BatchEngine(probs, tune=False)
+    be.plan()
+    be.step(graph=False)
+    be.check()
+    res = [be.results(i) for i in range(len(probs))]
+    for p, (f, g) in zip(probs, res):
+        fo, go = Oracle.from_problem(p).outprod(p.x, nthreads=8)
+        assert abs(f - fo) < TOL_E and normwise(g, go) < TOL_G
+        fs, gs = Engine(p).outprod(p.x)
+        assert abs(f - fs) < 1e-12 * abs(fs) and normwise(g, gs) < 1e-12
+    # one instance alone, then a different subset in another order: bitwise equal
+    be.plan([2])
+    be.step(graph=True)
+    be.check()
+    f2, g2 = be.results(2)
+    assert f2 == res[2][0] and np.array_equal(g2, res[2][1])
+    be.plan([4, 2, 0])
+    be.step(graph=True)
+    be.check()
+    for i in (4, 2, 0):
+        fi, gi = be.results(i)
+        assert fi == res[i][0] and np.array_equal(gi, res[i][1])
+
+
+def test_batch_graph_replay_tracks_new_inputs(torch_cuda):
+    from nbo_correlatedgaussians_b200.batch import BatchEngine
+    probs = _mixed(10)
+    be = BatchEngine(probs, tune=False)
+    be.plan()
+    be.step(graph=True)
+    be.check()
+    rng = np.random.default_rng(1)
+    for i, p in enumerate(probs):
+        x = p.x.copy()
+        x[p.siv:] = rng.normal(size=p.K)
+        be.set_x(i, x)
+        p.C = x[p.siv:]
+    be.step(graph=True)
+    be.check()
+    for i, p in enumerate(probs):
+        f, g = be.results(i)
+        fo, go = Oracle.from_problem(p).outprod(p.x, nthreads=8)
+        assert abs(f - fo) < TOL_E and normwise(g, go) < TOL_G
+
+
+def test_server_results_alone_and_in_mix(torch_cuda):
+    from nbo_correlatedgaussians_b200.serve import Server
+    probs = _mixed(20)
+    rng = np.random.default_rng(3)
+    xs = [[p.x + 1e-3 * rng.normal(size=p.x.size) for _ in range(3)] for p in probs]
+    # alone
+    alone = []
+    with Server(budget_bytes=8e9, max_slots=8, tune=False) as srv:
+        for p, xl in zip(probs, xs):
+            run = srv.open_run(p)
+            alone.append([srv.evaluate(run, x) for x in xl])
+            srv.close_run(run)
+    # all runs concurrently
+    mix = [None] * len(probs)
+    with Server(budget_bytes=8e9, max_slots=8, tune=False) as srv:
+        def client(i):
+            run = srv.open_run(probs[i])
+            mix[i] = [srv.evaluate(run, x) for x in xs[i]]
+            srv.close_run(run)
+        th = [threading.Thread(target=client, args=(i,)) for i in range(len(probs))]
+        for t in th:
+            t.start()
+        for t in th:
+            t.join()
+        st = srv.stats()
+    assert st["requests"] == 15 and st["p99_ms"] >= st["p50_ms"] > 0
+    for a, m in zip(alone, mix):
+        for (fa, ga), (fm, gm) in zip(a, m):
+            assert fa == fm and np.array_equal(ga, gm)
+
+
+def test_server_admission_under_budget(torch_cuda):
+    """A budget that fits one run at a time: runs are admitted one after another
+    as earlier runs close, and every run completes."""
+    from nbo_correlatedgaussians_b200 import synth
+    from nbo_correlatedgaussians_b200.serve import Server, workspace_estimate
+    probs = [synth.make_problem("He", 64, 30 + i) for i in range(3)]
+    budget = 1.5 * max(workspace_estimate(p) for p in probs)
+    order = []
+    with Server(budget_bytes=budget, max_slots=4, tune=False) as srv:
+        def client(i):
+            run = srv.open_run(probs[i])
+            order.append(("in", i, srv.used))
+            srv.evaluate(run, probs[i].x)
+            order.append(("out", i))
+            srv.close_run(run)
+        th = [threading.Thread(target=client, args=(i,)) for i in range(3)]
+        for t in th:
+            t.start()
+        for t in th:
+            t.join()
+    assert all(u <= budget for tag, *rest in order if tag == "in" for u in [rest[1]])
+    assert len([o for o in order if o[0] == "out"]) == 3
+    with pytest.raises(MemoryError):
+        with Server(budget_bytes=1e3, max_slots=1, tune=False) as srv:
+            srv.open_run(probs[0])

@@ -80,7 +80,7 @@ def test_oldquit_file_and_eigen_coefficients(torch_cuda):
     H, S, Kin, Pot, fb = eng.build_matrices(p.iv, p.C)
     assert normwise(H.cpu().numpy(), d["H"]) < 1e-12
     assert normwise(S.cpu().numpy(), d["S"]) < 1e-12
-    assert abs(float(fb.item()) - 4.296758204100342) < TOL_E
+    assert abs(float(fb[0].item()) - 4.296758204100342) < TOL_E
 
 
 @pytest.mark.parametrize("system,K", [("He", 64), ("H2", 64), ("LiH", 40)])
