@@ -2,8 +2,12 @@
 is exercised on (He, H2, LiH in non-Born-Oppenheimer internal coordinates).
 
 A symmetry term is a coordinate map ``sml`` (n x n, acting on the internal
-coordinates of the ket, python/matel.py:76-77), its shift map
-``sms = kron(sml^T, I3)`` (python/matel.py:87) and a weight ``scvv``.  The
+coordinates of the ket, python/matel.py:76-77), its shift map ``sms``
+(python/matel.py:87) and a weight ``scvv``.  The reference's Gaussians are
+centred, exp(-(r - s)^T (A x I3) (r - s)) (python/matel.py:125-136), so
+evaluating one at P r moves A to P^T A P and the centre s to P^-1 s: the shift
+map is kron(P^-1, I3).  For the permutations of oldquit.dat P^-1 = P^T, which
+is the kron(sml^T, I3) stored there.  The
 reference reads these from the input file (python/read_input.py:139-157) and
 ships them only for LiH (``oldquit.dat``); the He and H2 sets here are built
 the same way.
@@ -48,7 +52,8 @@ def mass_matrix(m0: float, masses) -> np.ndarray:
 
 
 def _sms_from_sml(sml: np.ndarray) -> np.ndarray:
-    return np.stack([np.kron(p.T, np.eye(3)) for p in sml])
+    """Shift maps kron(P^-1, I3) of the coordinate maps P (see the module doc)."""
+    return np.stack([np.kron(np.linalg.inv(p), np.eye(3)) for p in sml])
 
 
 def _perm_matrix(n: int, perm) -> np.ndarray:

@@ -46,6 +46,30 @@ def test_symmetry_sets_closed_under_inverse(system, nst):
         assert abs(abs(np.linalg.det(m)) - 1.0) < 1e-12
 
 
+@pytest.mark.parametrize("system", ["He", "H2", "LiH"])
+def test_symmetry_sets_make_H_bra_ket_symmetric(system):
+    """The reference's gradient (python/make_grad.py:61-79) assumes H_ij computed
+    with bra i equals H_ji computed with bra j; a symmetry set whose shift maps
+    do not match its coordinate maps breaks that.  Checked with the oracle."""
+    from oracle.oracle import Oracle
+    p = synth.make_problem(system, 5, 3)
+    o = Oracle.from_problem(p)
+    for i in range(2, 6):
+        for j in range(1, i):
+            a = sum(w * np.array(o.matel(p.iv, s + 1, i, j)) for s, w in enumerate(p.scvv))
+            b = sum(w * np.array(o.matel(p.iv, s + 1, j, i)) for s, w in enumerate(p.scvv))
+            assert abs(a[0] - b[0]) < 1e-12 * abs(a[0])
+            ha, hb = a[1] + a[2] - a[3], b[1] + b[2] - b[3]
+            assert abs(ha - hb) < 1e-11 * abs(ha)
+
+
+def test_shift_maps_are_inverse_coordinate_maps():
+    for system in ("He", "H2", "LiH"):
+        sml, sms, _ = symmetry_set(system)
+        for P, Sm in zip(sml, sms):
+            np.testing.assert_allclose(Sm, np.kron(np.linalg.inv(P), np.eye(3)), atol=1e-15)
+
+
 def test_h2_proton_swap_is_involution():
     sml, _, _ = symmetry_set("H2")
     for m in sml:
