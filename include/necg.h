@@ -156,6 +156,25 @@ int necg_batch_replay(necg_batch *b, void *stream);
  * first non-OK code or NECG_OK. */
 int necg_batch_status(necg_batch *b, int *status_out, void *stream);
 
+/* necg_outprod for callers that cannot allocate device memory (a host that
+ * gives the GPU to its own fixed memory pool at start-up, a loop that cannot
+ * afford an allocation's implicit synchronisation, a foreign-language driver
+ * linking only this C ABI).  It allocates nothing: every intermediate lives in
+ * one 32 MiB scratch array defined at file scope in the library, which every GPU
+ * that loads the library holds until the process exits.  The caller passes the
+ * problem constants as host arrays (layouts as for necg_create) and x, f, g in
+ * device memory.  Synchronous: it returns the pair status of this evaluation.
+ * A problem whose intermediates do not fit the 32 MiB returns
+ * NECG_ERR_CAPACITY: K <= 784 for n = 5, nst = 24 (LiH); K <= 1144 for n = 3,
+ * nst = 4 (H2); K <= 1247 for n = 2, nst = 2 (He).  The first call on a device looks up the array's device address and
+ * must come before any stream capture on that device.  Calls share the array,
+ * so calls that overlap on the GPU race; callers serialise them.  No counterpart
+ * in the reference: its outprod (python/outprod.py:20) allocates as NumPy does. */
+int necg_outprod_noalloc(int n, int nst, int K, double efs, const double *mass_host,
+                         const double *ncv_host, const double *scvv_host, const double *sml_host,
+                         const double *sms_host, const double *x_dev, double *f_dev, double *g_dev,
+                         void *stream);
+
 /* Synchronise the handle's last stream and report the pair status of the most
  * recent evaluation: NECG_OK, NECG_ERR_NOT_PD or NECG_ERR_NONFINITE; *bad_pair
  * (may be NULL) receives the first failing pair as k*K + l, or -1. */

@@ -40,6 +40,7 @@ SIGNATURES = [
     ("necg_matel", _i, [_vp, _i, _vp, _i, _vp, _vp, _vp]),
     ("necg_gradel", _i, [_vp, _i, _vp, _i, _vp, _vp, _vp, _vp]),
     ("necg_f0", _i, [_vp, _i, _vp, _vp, _vp]),
+    ("necg_outprod_noalloc", _i, [_i, _i, _i, _d, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     ("necg_status", _i, [_vp, ctypes.POINTER(_ll)]),
     ("necg_batch_create", _i, [_i, _i, ctypes.POINTER(_vp)]),
     ("necg_batch_destroy", _i, [_vp]),
