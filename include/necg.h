@@ -66,8 +66,19 @@ int necg_set_tiles(necg_handle *h, int lc_energy, int lc_grad);
 /* Register-budget variant of the energy and gradient tile kernels (one warp
  * per block): the minimum number of resident warps per SM the kernel is
  * compiled for, one of 8, 12, 16, 20 (2, 3, 4, 5 warps per scheduler: up to
- * 255, 168, 128, 96 registers per thread).  Set by the autotuner. */
+ * 255, 168, 128, 96 registers per thread).  The gradient kernel also has
+ * 112 and 116: 12 and 16 warps per SM with its per-lane accumulators held in
+ * shared memory instead of registers.  Set by the autotuner. */
 int necg_set_variant(necg_handle *h, int minw_energy, int minw_grad);
+
+/* Gradient pass over unordered pairs: each (k >= l, P) term yields the bra
+ * gradient for k and the ket gradient for l, halving the terms of the ordered
+ * pass (which follows python/make_grad.py:37-55 and evaluates every ordered
+ * pair).  Needs a symmetry set closed under inverse (each sml and sms has its
+ * inverse in the set) and n <= 5; otherwise NECG_ERR_UNSUPPORTED and the ordered
+ * pass stays in use.  On by default when available.  lc: kets per tile (1..64);
+ * minw: 8, 12 or 16 warps per SM.  Set by the autotuner. */
+int necg_set_symmetric(necg_handle *h, int enable, int lc, int minw);
 
 /* One objective evaluation: python/outprod.py:20-76 outprod(x) -> (f, g),
  * including make_grad (python/make_grad.py:18-90).  Device pointers; H_dev and
@@ -165,7 +176,7 @@ int necg_batch_status(necg_batch *b, int *status_out, void *stream);
  * problem constants as host arrays (layouts as for necg_create) and x, f, g in
  * device memory.  Synchronous: it returns the pair status of this evaluation.
  * A problem whose intermediates do not fit the 32 MiB returns
- * NECG_ERR_CAPACITY: K <= 784 for n = 5, nst = 24 (LiH); K <= 1144 for n = 3,
+ * NECG_ERR_CAPACITY: K <= 779 for n = 5, nst = 24 (LiH); K <= 1143 for n = 3,
  * nst = 4 (H2); K <= 1247 for n = 2, nst = 2 (He).  The first call on a device looks up the array's device address and
  * must come before any stream capture on that device.  Calls share the array,
  * so calls that overlap on the GPU race; callers serialise them.  No counterpart

@@ -13,6 +13,9 @@ The search space:
          per block): 8 -> up to 255 registers per thread, 12 -> 168, 16 -> 128,
          20 -> 96 (the register file is split between the four schedulers, so
          these are the only distinct budgets)
+  sym    gradient pass over unordered pairs (bra and ket gradient per term,
+         when the symmetry set is closed under inverse) instead of ordered
+         pairs, with its own ket chunk lc_s and variant minw_s
 """
 from __future__ import annotations
 
@@ -31,6 +34,9 @@ CACHE = os.environ.get("NECG_TUNE_CACHE", os.path.join(os.path.dirname(os.path.a
 LC_E = (2, 4, 8, 16, 32)
 LC_G = (4, 8, 16, 32, 64)
 MINB = (8, 12, 16, 20)
+MINB_GRAD_EXTRA = (112, 116)  # gradient kernel with shared-memory accumulators
+LC_S = (2, 4, 8, 16)          # kets per tile of the symmetric gradient pass
+MINW_SYM = (8, 12)
 
 
 def _bucket(K: int) -> int:
@@ -79,23 +85,37 @@ def tune(eng: Engine, x, K: int, reps: int = 3, report: bool = False) -> dict:
     L = eng.L
     x = eng._tensor(x)
     _lib.check(L.necg_profile(eng.h, 1), "necg_profile")
+    L.necg_set_symmetric(eng.h, 0, 4, 8)
     rows = []
     best_e = (float("inf"), None)
     best_g = (float("inf"), None)
-    for minb in MINB:
+    for minb in MINB + MINB_GRAD_EXTRA:
         for lc_e, lc_g in zip(LC_E, LC_G):
             _lib.check(L.necg_set_tiles(eng.h, lc_e, lc_g), "necg_set_tiles")
-            _lib.check(L.necg_set_variant(eng.h, minb, minb), "necg_set_variant")
+            _lib.check(L.necg_set_variant(eng.h, minb if minb < 100 else 8, minb), "necg_set_variant")
             _phase_times(eng, x, K, 1)  # warm-up (also builds the energy tile list)
             t = _phase_times(eng, x, K, reps).min(axis=0)
             e_ms, g_ms = float(t[1]), float(t[3] + t[4])
             rows.append({"minb": minb, "lc_e": lc_e, "lc_g": lc_g, "energy_ms": e_ms, "grad_ms": g_ms})
-            if e_ms < best_e[0]:
+            if e_ms < best_e[0] and minb < 100:
                 best_e = (e_ms, (lc_e, minb))
             if g_ms < best_g[0]:
                 best_g = (g_ms, (lc_g, minb))
     res = {"lc_e": best_e[1][0], "minb_e": best_e[1][1], "lc_g": best_g[1][0], "minb_g": best_g[1][1],
-           "energy_ms": best_e[0], "grad_ms": best_g[0]}
+           "energy_ms": best_e[0], "grad_ms": best_g[0], "sym": 0, "lc_s": 4, "minw_s": 8}
+    # the symmetric gradient pass (unordered pairs), when the symmetry set allows it
+    if L.necg_set_symmetric(eng.h, 1, 4, 8) == _lib.NECG_OK:
+        _lib.check(L.necg_set_tiles(eng.h, res["lc_e"], res["lc_g"]), "necg_set_tiles")
+        _lib.check(L.necg_set_variant(eng.h, res["minb_e"], res["minb_g"]), "necg_set_variant")
+        for minw in MINW_SYM:
+            for lc in LC_S:
+                _lib.check(L.necg_set_symmetric(eng.h, 1, lc, minw), "necg_set_symmetric")
+                _phase_times(eng, x, K, 1)
+                t = _phase_times(eng, x, K, reps).min(axis=0)
+                g_ms = float(t[3] + t[4])
+                rows.append({"sym": 1, "minw": minw, "lc_s": lc, "grad_ms": g_ms})
+                if g_ms < res["grad_ms"]:
+                    res.update(grad_ms=g_ms, sym=1, lc_s=lc, minw_s=minw)
     if report:
         res["table"] = rows
     apply(eng, res)
@@ -105,6 +125,10 @@ def tune(eng: Engine, x, K: int, reps: int = 3, report: bool = False) -> dict:
 def apply(eng: Engine, cfg: dict) -> None:
     _lib.check(eng.L.necg_set_tiles(eng.h, int(cfg["lc_e"]), int(cfg["lc_g"])), "necg_set_tiles")
     _lib.check(eng.L.necg_set_variant(eng.h, int(cfg["minb_e"]), int(cfg["minb_g"])), "necg_set_variant")
+    sym = int(cfg.get("sym", 0))
+    rc = eng.L.necg_set_symmetric(eng.h, sym, int(cfg.get("lc_s", 4)), int(cfg.get("minw_s", 8)))
+    if rc != _lib.NECG_OK and sym:
+        _lib.check(rc, "necg_set_symmetric")
 
 
 def tuned(eng: Engine, x, K: int, retune: bool = False) -> dict:

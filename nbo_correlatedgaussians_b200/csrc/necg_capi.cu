@@ -58,7 +58,8 @@ void free_all(necg_handle *h) {
         if (e) cudaEventDestroy(e);
     void *ptrs[] = {h->d_sml, h->d_sms, h->d_scvv, h->d_bra, h->d_ket, h->d_part, h->d_H,
                     h->d_S, h->d_rows, h->d_scal, h->d_x, h->d_g, h->d_f, h->d_status,
-                    h->d_tiles};
+                    h->d_tiles, h->d_pinv, h->d_kcnt, h->d_ksrc, h->d_kcoef, h->d_stiles,
+                    h->d_stile_start, h->d_psym};
     for (void *p : ptrs)
         if (p) cudaFree(p);
 }
@@ -83,6 +84,118 @@ int ensure_tiles(necg_handle *h, int K, cudaStream_t st) {
     h->tiles_K = K;
     h->tiles_lc = h->lc_e;
     h->ntiles = (int)t.size();
+    return NECG_OK;
+}
+
+// Lower-triangle tiles of chunk LC for the symmetric pass, plus the first tile
+// of each 32-row block; the partial buffer grows here if this K and LC need more.
+int ensure_sym_tiles(necg_handle *h, int K, cudaStream_t st) {
+    if (h->stiles_K == K && h->stiles_lc == h->lc_s) return NECG_OK;
+    std::vector<int2> t;
+    std::vector<int> start;
+    const int nkb = (K + 31) / 32, LC = h->lc_s;
+    for (int kb = 0; kb < nkb; ++kb) {
+        start.push_back((int)t.size());
+        const int last = kb * 32 + 31 < K - 1 ? kb * 32 + 31 : K - 1;
+        for (int lc = 0; lc <= last / LC; ++lc) t.push_back(make_int2(kb, lc));
+    }
+    start.push_back((int)t.size());
+    if ((int)t.size() > h->stiles_cap) {
+        if (h->d_stiles) cudaFree(h->d_stiles);
+        h->d_stiles = nullptr;
+        CK(cudaMalloc((void **)&h->d_stiles, t.size() * sizeof(int2)));
+        h->stiles_cap = (int)t.size();
+    }
+    if (!h->d_stile_start) CK(cudaMalloc((void **)&h->d_stile_start, ((h->K_max + 31) / 32 + 2) * sizeof(int)));
+    const int PS = necg::part_stride(h->n);
+    const size_t need = t.size() * (size_t)PS * (32 + LC);
+    if (need > h->psym_cap) {
+        if (h->d_psym) cudaFree(h->d_psym);
+        h->d_psym = nullptr;
+        CK(cudaMalloc((void **)&h->d_psym, need * sizeof(double)));
+        h->ws_bytes += (long long)((need - h->psym_cap) * sizeof(double));
+        h->psym_cap = need;
+    }
+    CK(cudaMemcpyAsync(h->d_stiles, t.data(), t.size() * sizeof(int2), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(h->d_stile_start, start.data(), start.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+    CK(cudaStreamSynchronize(st));
+    h->stiles_K = K;
+    h->stiles_lc = LC;
+    h->nstiles = (int)t.size();
+    return NECG_OK;
+}
+
+// Inverse of each symmetry term (sml and sms both inverted) and the map of a
+// ket gradient from P's frame to the basis function's frame.  Sets sym_ok
+// when every term's inverse is in the set and n <= 5.
+int setup_symmetric(necg_handle *h) {
+    const int n = h->n, nst = h->nst, m = 3 * n;
+    if (n > 5) return NECG_OK;
+    std::vector<int> pinv(nst, -1);
+    for (int p = 0; p < nst; ++p)
+        for (int q = 0; q < nst && pinv[p] < 0; ++q) {
+            bool ok = true;
+            for (int i = 0; i < n && ok; ++i)
+                for (int j = 0; j < n && ok; ++j) {
+                    double s = 0.0;
+                    for (int k = 0; k < n; ++k) s += h->sml[(size_t)p * n * n + i * n + k] * h->sml[(size_t)q * n * n + k * n + j];
+                    ok = fabs(s - (i == j ? 1.0 : 0.0)) < 1e-12;
+                }
+            for (int i = 0; i < m && ok; ++i)
+                for (int j = 0; j < m && ok; ++j) {
+                    double s = 0.0;
+                    for (int k = 0; k < m; ++k) s += h->sms[(size_t)p * m * m + i * m + k] * h->sms[(size_t)q * m * m + k * m + j];
+                    ok = fabs(s - (i == j ? 1.0 : 0.0)) < 1e-12;
+                }
+            if (ok) pinv[p] = q;
+        }
+    for (int p = 0; p < nst; ++p)
+        if (pinv[p] < 0) return NECG_OK;  // not closed under inverse: ordered pass only
+    const int T = n * (n + 1) / 2, PS = T + 1 + m;
+    std::vector<std::vector<std::pair<int, double>>> rows((size_t)nst * PS);
+    for (int p = 0; p < nst; ++p) {
+        const double *P = &h->sml[(size_t)p * n * n];
+        const double *Sm = &h->sms[(size_t)p * m * m];
+        for (int a = 0; a < n; ++a)
+            for (int b = 0; b <= a; ++b) {  // (sml G' sml^T)_ab
+                std::vector<double> coef(T, 0.0);
+                for (int cc = 0; cc < n; ++cc)
+                    for (int d = 0; d < n; ++d) coef[necg::sx(cc, d)] += P[a * n + cc] * P[b * n + d];
+                auto &row = rows[(size_t)p * PS + necg::sx(a, b)];
+                for (int s = 0; s < T; ++s)
+                    if (coef[s] != 0.0) row.push_back({s, coef[s]});
+            }
+        rows[(size_t)p * PS + T].push_back({T, 1.0});
+        for (int r = 0; r < m; ++r) {  // (sms^T g')_r
+            auto &row = rows[(size_t)p * PS + T + 1 + r];
+            for (int cc = 0; cc < m; ++cc)
+                if (Sm[cc * m + r] != 0.0) row.push_back({T + 1 + cc, Sm[cc * m + r]});
+        }
+    }
+    int maxnz = 1;
+    for (auto &r : rows) maxnz = (int)r.size() > maxnz ? (int)r.size() : maxnz;
+    std::vector<int> cnt(rows.size()), src(rows.size() * maxnz, 0);
+    std::vector<double> coef(rows.size() * maxnz, 0.0);
+    for (size_t e = 0; e < rows.size(); ++e) {
+        cnt[e] = (int)rows[e].size();
+        for (size_t i = 0; i < rows[e].size(); ++i) {
+            src[e * maxnz + i] = rows[e][i].first;
+            coef[e * maxnz + i] = rows[e][i].second;
+        }
+    }
+    int rc = NECG_OK;
+    if (!rc) rc = dalloc(h, &h->d_pinv, (size_t)nst);
+    if (!rc) rc = dalloc(h, &h->d_kcnt, cnt.size());
+    if (!rc) rc = dalloc(h, &h->d_ksrc, src.size());
+    if (!rc) rc = dalloc(h, &h->d_kcoef, coef.size());
+    if (rc) return rc;
+    CK(cudaMemcpy(h->d_pinv, pinv.data(), nst * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(h->d_kcnt, cnt.data(), cnt.size() * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(h->d_ksrc, src.data(), src.size() * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(h->d_kcoef, coef.data(), coef.size() * sizeof(double), cudaMemcpyHostToDevice));
+    h->kmaxnz = maxnz;
+    h->sym_ok = true;
+    h->use_sym = true;
     return NECG_OK;
 }
 
@@ -111,7 +224,41 @@ LaunchArgs base_args(necg_handle *h, int K) {
     a.part = h->d_part;
     a.status = h->d_status;
     a.lam = 1.0;
+    a.pinv = h->d_pinv;
+    a.kmap = necg::KetMap{h->d_kcnt, h->d_ksrc, h->d_kcoef, h->kmaxnz};
+    a.stiles = h->d_stiles;
+    a.stile_start = h->d_stile_start;
+    a.nstiles = h->nstiles;
+    a.LC_s = h->lc_s;
+    a.minb_s = h->minb_s;
+    a.psym = h->d_psym;
     return a;
+}
+
+// The gradient passes after E and norm are in scal: symmetric (unordered pairs)
+// when available, ordered otherwise.
+int launch_gradient(necg_handle *h, LaunchArgs &a, cudaStream_t st) {
+    if (h->use_sym) {
+        int rc = ensure_sym_tiles(h, a.K, st);
+        if (rc) return rc;
+        a.stiles = h->d_stiles;
+        a.stile_start = h->d_stile_start;
+        a.nstiles = h->nstiles;
+        a.LC_s = h->lc_s;
+        a.psym = h->d_psym;
+        mark(h, 3, st);
+        necg::launch_gsym(a, st);
+        mark(h, 4, st);
+        necg::launch_gsym_reduce(a, st);
+        mark(h, 5, st);
+        return NECG_OK;
+    }
+    mark(h, 3, st);
+    necg::launch_grad_tiles(a, st);
+    mark(h, 4, st);
+    necg::launch_grad_reduce(a, st);
+    mark(h, 5, st);
+    return NECG_OK;
 }
 
 int check_K(necg_handle *h, int K) {
@@ -180,6 +327,7 @@ int necg_create(int n, int nst, int K_max, double efs, const double *mass_host,
     if (!rc) rc = cuda_fail(cudaMemcpy(h->d_sms, h->sms.data(), h->sms.size() * 8, cudaMemcpyHostToDevice));
     if (!rc) rc = cuda_fail(cudaMemcpy(h->d_scvv, h->scvv.data(), h->scvv.size() * 8, cudaMemcpyHostToDevice));
     if (!rc) rc = cuda_fail(cudaMemset(h->d_status, 0, 16));
+    if (!rc) rc = setup_symmetric(h);
     if (rc) {
         free_all(h);
         delete h;
@@ -207,9 +355,19 @@ int necg_set_tiles(necg_handle *h, int lc_energy, int lc_grad) {
     return NECG_OK;
 }
 
+int necg_set_symmetric(necg_handle *h, int enable, int lc, int minw) {
+    if (!h || lc < 1 || lc > 64 || !(minw == 8 || minw == 12 || minw == 16)) return NECG_ERR_ARG;
+    if (enable && !h->sym_ok) return NECG_ERR_UNSUPPORTED;
+    h->use_sym = enable != 0;
+    h->lc_s = lc;
+    h->minb_s = minw;
+    return NECG_OK;
+}
+
 int necg_set_variant(necg_handle *h, int minw_energy, int minw_grad) {
     auto okw = [](int w) { return w == 8 || w == 12 || w == 16 || w == 20; };
-    if (!h || !okw(minw_energy) || !okw(minw_grad)) return NECG_ERR_ARG;
+    if (!h || !okw(minw_energy) || !(okw(minw_grad) || minw_grad == 112 || minw_grad == 116))
+        return NECG_ERR_ARG;
     h->minb_e = minw_energy;
     h->minb_g = minw_grad;
     return NECG_OK;
@@ -252,17 +410,14 @@ int necg_outprod(necg_handle *h, int K, const double *x_dev, double *f_dev, doub
     a.H = H_dev ? H_dev : h->d_H;
     a.S = S_dev ? S_dev : h->d_S;
     a.g = g_dev;
+    if (h->use_sym && (rc = ensure_sym_tiles(h, K, st))) return rc;
     mark(h, 0, st);
     if (necg::launch_prep(a, st)) return NECG_ERR_UNSUPPORTED;
     mark(h, 1, st);
     necg::launch_energy(a, st);
     mark(h, 2, st);
     necg::launch_rows_finalize(a, f_dev, g_dev + siv, 0, 0.0, 0.0, st);
-    mark(h, 3, st);
-    necg::launch_grad_tiles(a, st);
-    mark(h, 4, st);
-    necg::launch_grad_reduce(a, st);
-    mark(h, 5, st);
+    if ((rc = launch_gradient(h, a, st))) return rc;
     return finish_launch();
 }
 
@@ -301,7 +456,7 @@ int necg_make_grad(necg_handle *h, int K, const double *iv_dev, const double *C_
     // GRADC = 2 norm (H - eng S) C with the caller's eng and norm; also sets
     // the E and norm the gradient tiles read
     necg::launch_rows_finalize(a, nullptr, g_dev + siv, 1, eng, norm, st);
-    necg::launch_grad(a, st);
+    if ((rc = launch_gradient(h, a, st))) return rc;
     return finish_launch();
 }
 
@@ -322,7 +477,7 @@ int necg_make_grad_dev(necg_handle *h, int K, const double *iv_dev, const double
     a.g = g_dev;
     if (necg::launch_prep(a, st)) return NECG_ERR_UNSUPPORTED;
     necg::launch_rows_finalize(a, nullptr, g_dev + siv, 2, 0.0, 0.0, st, en_dev, nullptr);
-    necg::launch_grad(a, st);
+    if ((rc = launch_gradient(h, a, st))) return rc;
     return finish_launch();
 }
 

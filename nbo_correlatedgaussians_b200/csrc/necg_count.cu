@@ -74,8 +74,10 @@ template <int N> void count_term(int which, long long &flops, long long &special
         h += w * ov * (2.0 * tau + rho - sig);
         s += w * ov;
     } else {
-        CD accG[tri(N)], accS[3 * N], accD;
-        term_grad<N>(b, kr, cs, CD(1.0), CD(0.5), CD(1.0), accG, accD, accS);
+        RegAcc<N, CD> acc;
+        acc.zero();
+        count_ctx() = CountCtx();  // zeroing the accumulators is not part of a term
+        term_grad<N>(b, kr, cs, CD(1.0), CD(0.5), CD(1.0), acc);
     }
     flops = count_ctx().flops;
     special = count_ctx().special;

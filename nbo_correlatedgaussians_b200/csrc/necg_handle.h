@@ -25,4 +25,16 @@ struct necg_handle {
     long long ws_bytes = 0;
     bool profile = false;
     cudaEvent_t ev[6] = {};
+    // symmetric gradient pass (when the symmetry set is closed under inverse)
+    bool sym_ok = false, use_sym = false;
+    int lc_s = 4, minb_s = 8;
+    int *d_pinv = nullptr;
+    int *d_kcnt = nullptr, *d_ksrc = nullptr;
+    double *d_kcoef = nullptr;
+    int kmaxnz = 0;
+    int2 *d_stiles = nullptr;
+    int *d_stile_start = nullptr;
+    int stiles_cap = 0, stiles_K = -1, stiles_lc = -1, nstiles = 0;
+    double *d_psym = nullptr;
+    size_t psym_cap = 0;  // doubles
 };

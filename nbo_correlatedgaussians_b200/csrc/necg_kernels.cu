@@ -29,6 +29,19 @@ struct DevKet {
     __device__ __forceinline__ const double *at(size_t off) const { return p + off; }
 };
 
+// Gradient accumulators of one lane in shared memory, interleaved by lane
+// (field t of lane j at t * 32 + j): conflict-free, and not held in registers.
+template <int N> struct SmemAcc {
+    double *p;  // shared base + lane
+    __device__ __forceinline__ void zero() {
+#pragma unroll
+        for (int t = 0; t < Part<N>::size; ++t) p[t * 32] = 0.0;
+    }
+    __device__ __forceinline__ double &g(int t) { return p[t * 32]; }
+    __device__ __forceinline__ double &d() { return p[tri(N) * 32]; }
+    __device__ __forceinline__ double &s(int t) { return p[(tri(N) + 1 + t) * 32]; }
+};
+
 // Status word: [0] bit flags, [1] first failing pair (row-major k*K + l).
 __device__ __forceinline__ void flag_status(int *status, int flags, int pair) {
     if (!flags) return;
@@ -49,9 +62,10 @@ __global__ void __launch_bounds__(128) prep_ket_kernel(const double *__restrict_
                                                        Consts<N> cs, const double *__restrict__ sml,
                                                        const double *__restrict__ sms,
                                                        const double *__restrict__ scvv,
-                                                       double *__restrict__ ket) {
+                                                       double *__restrict__ ket,
+                                                       const int *__restrict__ pinv) {
     const int id = blockIdx.x * blockDim.x + threadIdx.x;
-    if (id < K * nst) prep_ket_one<N>(iv, C, nst, cs, sml, sms, scvv, ket, id);
+    if (id < K * nst) prep_ket_one<N>(iv, C, nst, cs, sml, sms, scvv, ket, id, pinv);
 }
 
 // Energy tiles over the lower triangle (the loop of python/outprod.py:49-54 and
@@ -176,7 +190,8 @@ __global__ void __launch_bounds__(1024) finalize_kernel(const double *__restrict
 // python/make_grad.py:37-55, contracted with C on the fly as lines 61-79 do).
 // Tile t = (kb, lc); lane k accumulates over l in the chunk and all P and
 // writes its partial to part[(lc * Part::size + f) * K + k].
-template <int N, int MINW>
+// SACC: accumulators in shared memory instead of registers.
+template <int N, int MINW, bool SACC>
 __global__ void __launch_bounds__(32, MINW) grad_kernel(int nkb, int nlc, int LC, int K, int nst,
                                                    Consts<N> cs, const double *__restrict__ bra,
                                                    const double *__restrict__ ket,
@@ -187,9 +202,115 @@ __global__ void __launch_bounds__(32, MINW) grad_kernel(int nkb, int nlc, int LC
     if (warp >= nkb * nlc) return;
     int k, lc, l0, l1;
     if (!grad_lane_range(warp, lane, nkb, LC, K, k, lc, l0, l1)) return;
-    const bool ok = grad_lane<N, double>(BraRef{bra + k, (size_t)K}, DevKet{ket}, l0, l1, nst, cs, lam,
-                                         scal[0], part + (size_t)lc * Part<N>::size * K + k, (size_t)K);
+    double *out = part + (size_t)lc * Part<N>::size * K + k;
+    bool ok;
+    if (SACC) {
+        __shared__ double sacc[Part<N>::size * 32];
+        SmemAcc<N> acc{sacc + lane};
+        ok = grad_lane<N, double>(BraRef{bra + k, (size_t)K}, DevKet{ket}, l0, l1, nst, cs, lam, scal[0],
+                                  out, (size_t)K, acc);
+    } else {
+        ok = grad_lane<N, double>(BraRef{bra + k, (size_t)K}, DevKet{ket}, l0, l1, nst, cs, lam, scal[0],
+                                  out, (size_t)K);
+    }
     if (!ok) flag_status(status, 1, k * K + l0);
+}
+
+
+// ---------------------------------------------------------------------------
+// Symmetric gradient tiles: each unordered pair (k >= l) once.  Tile (kb, lc)
+// of the lower-triangle tile list; lane = bra k.  For every ket (l, P) the
+// lane adds the bra gradient of its term to its shared-memory accumulator and
+// writes the term's ket gradient (in P's frame) to its row of a per-warp
+// table; the warp then sums the table column by column, each lane maps one
+// component back to l's frame (KetMap) and accumulates it over P.  Bra
+// partials: part_b[(t * PS + f) * 32 + lane]; ket partials:
+// part_k[(t * LC + l - l0) * PS + f].  Requires PS <= 32 (n <= 5).
+template <int N, int MINW>
+__global__ void __launch_bounds__(32, MINW) gsym_kernel(const int2 *__restrict__ tiles, int ntiles,
+                                                   int LC, int K, int nst, Consts<N> cs,
+                                                   const double *__restrict__ bra,
+                                                   const double *__restrict__ ket,
+                                                   const double *__restrict__ C,
+                                                   const double *__restrict__ scal, KetMap kmap,
+                                                   double *__restrict__ part_b,
+                                                   double *__restrict__ part_k, int *status) {
+    using KL = KetLayout<N>;
+    constexpr int PS = Part<N>::size;
+    static_assert(PS <= 32, "the symmetric pass needs tri(n) + 1 + 3n <= 32");
+    __shared__ double sacc[PS * 32];
+    __shared__ double krow[32 * 33];
+    __shared__ double kred[32];
+    const int t = blockIdx.x;
+    const int lane = threadIdx.x;
+    if (t >= ntiles) return;
+    const int2 tl = tiles[t];
+    const int k = tl.x * 32 + lane;
+    const int l0 = tl.y * LC;
+    const int l1 = min(l0 + LC, K);
+    const bool kval = k < K;
+    const double E = scal[0];
+    const double Ck = kval ? C[k] : 0.0;
+    SmemAcc<N> acc{sacc + lane};
+    acc.zero();
+    const BraRef b{bra + (kval ? k : 0), (size_t)K};
+    struct RowOut {
+        double *r;
+        __device__ __forceinline__ void put(int f, double v) { r[f] = v; }
+        __device__ __forceinline__ void add(int f, double v) { r[f] += v; }
+    } ko{krow + lane * 33};
+    bool ok = true;
+    for (int l = l0; l < l1; ++l) {
+        double accl = 0.0;
+        for (int P = 0; P < nst; ++P) {
+            const double *kr = ket + ((size_t)l * nst + P) * KL::size;
+            if (kval && l <= k) {
+                const double wk = l < k ? 2.0 * Ck * kr[KL::winv] : 0.0;
+                ok = term_sym<N, double>(b, kr, cs, E, kr[KL::wC], wk, acc, ko) && ok;
+            } else {
+#pragma unroll
+                for (int f = 0; f < PS; ++f) ko.r[f] = 0.0;
+            }
+            __syncwarp();
+            double v = 0.0;
+            if (lane < PS)
+#pragma unroll 8
+                for (int r = 0; r < 32; ++r) v += krow[r * 33 + lane];
+            kred[lane] = v;
+            __syncwarp();
+            if (lane < PS) accl += ket_map_apply(kmap, P, lane, PS, kred);
+            __syncwarp();
+        }
+        if (lane < PS) part_k[((size_t)t * LC + (l - l0)) * PS + lane] = accl;
+    }
+    if (kval) {
+#pragma unroll
+        for (int f = 0; f < PS; ++f) part_b[((size_t)t * PS + f) * 32 + lane] = sacc[f * 32 + lane];
+    }
+    if (!ok) flag_status(status, 1, k * K + l0);
+}
+
+// Sum the symmetric-pass partials of basis m into out[f * K + m]: its bra
+// partials from the tiles of block kb = m / 32 (lane m % 32) and its ket
+// partials from the tiles of chunk lc = m / LC in every block kb' >= that chunk.
+template <int N>
+__global__ void __launch_bounds__(256) gsym_sum_kernel(const int *__restrict__ tstart, int LC, int K,
+                                                       const double *__restrict__ part_b,
+                                                       const double *__restrict__ part_k,
+                                                       double *__restrict__ out) {
+    constexpr int PS = Part<N>::size;
+    const int id = blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= PS * K) return;
+    const int f = id / K, m = id - f * K;
+    const int kb = m >> 5, lane = m & 31;
+    double s = 0.0;
+    for (int t = tstart[kb]; t < tstart[kb + 1]; ++t) s += part_b[((size_t)t * PS + f) * 32 + lane];
+    const int lc = m / LC, ll = m - lc * LC;
+    const int nkb = (K + 31) >> 5;
+    int kb0 = lc * LC - 31;
+    kb0 = kb0 > 0 ? (kb0 + 31) >> 5 : 0;
+    for (int q = kb0; q < nkb; ++q) s += part_k[((size_t)(tstart[q] + lc) * LC + ll) * PS + f];
+    out[(size_t)f * K + m] = s;
 }
 
 // Sum the gradient-tile partials over the ket chunks, in place into chunk 0:
@@ -315,7 +436,7 @@ template <int N> struct Launch {
         prep_bra_kernel<N><<<(a.K + 127) / 128, 128, 0, st>>>(a.iv, a.K, cs, a.bra);
         const int nk = a.K * a.nst;
         prep_ket_kernel<N><<<(nk + 127) / 128, 128, 0, st>>>(a.iv, a.C, a.K, a.nst, cs, a.sml, a.sms,
-                                                             a.scvv, a.ket);
+                                                             a.scvv, a.ket, a.pinv);
     }
     template <int MINW> static void energy_v(const LaunchArgs &a, cudaStream_t st) {
         Consts<N> cs = make_consts<N>(a.mass_h, a.ncv_h, a.efs);
@@ -330,18 +451,22 @@ template <int N> struct Launch {
         default: energy_v<8>(a, st); break;
         }
     }
-    template <int MINW> static void grad_v(const LaunchArgs &a, cudaStream_t st) {
+    template <int MINW, bool SACC> static void grad_v(const LaunchArgs &a, cudaStream_t st) {
         Consts<N> cs = make_consts<N>(a.mass_h, a.ncv_h, a.efs);
         const int nkb = (a.K + 31) / 32, nlc = (a.K + a.LC_g - 1) / a.LC_g;
-        grad_kernel<N, MINW><<<nkb * nlc, 32, 0, st>>>(nkb, nlc, a.LC_g, a.K, a.nst, cs, a.bra, a.ket,
-                                                       a.scal, a.lam, a.part, a.status);
+        grad_kernel<N, MINW, SACC><<<nkb * nlc, 32, 0, st>>>(nkb, nlc, a.LC_g, a.K, a.nst, cs, a.bra,
+                                                             a.ket, a.scal, a.lam, a.part, a.status);
     }
+    // variant codes: 8, 12, 16, 20 = warps per SM with register accumulators;
+    // 112, 116 = 12, 16 warps per SM with shared-memory accumulators
     static void grad_tiles(const LaunchArgs &a, cudaStream_t st) {
         switch (a.minb_g) {
-        case 12: grad_v<12>(a, st); break;
-        case 16: grad_v<16>(a, st); break;
-        case 20: grad_v<20>(a, st); break;
-        default: grad_v<8>(a, st); break;
+        case 12: grad_v<12, false>(a, st); break;
+        case 16: grad_v<16, false>(a, st); break;
+        case 20: grad_v<20, false>(a, st); break;
+        case 112: grad_v<12, true>(a, st); break;
+        case 116: grad_v<16, true>(a, st); break;
+        default: grad_v<8, false>(a, st); break;
         }
     }
     static void grad_reduce(const LaunchArgs &a, cudaStream_t st) {
@@ -351,6 +476,31 @@ template <int N> struct Launch {
         if (nlc > 1) grad_sum_kernel<<<(unsigned)((nthr + 255) / 256), 256, 0, st>>>(a.part, nlc, a.K, PS);
         grad_reduce_kernel<N><<<(a.K + 127) / 128, 128, 0, st>>>(a.part, a.K, a.bra, a.C, a.scal, a.g,
                                                                   a.status);
+    }
+    template <int MINW> static void gsym_v(const LaunchArgs &a, cudaStream_t st) {
+        if constexpr (Part<N>::size <= 32) {
+            Consts<N> cs = make_consts<N>(a.mass_h, a.ncv_h, a.efs);
+            gsym_kernel<N, MINW><<<a.nstiles, 32, 0, st>>>(a.stiles, a.nstiles, a.LC_s, a.K, a.nst, cs, a.bra,
+                                                           a.ket, a.C, a.scal, a.kmap, a.psym,
+                                                           a.psym + (size_t)a.nstiles * Part<N>::size * 32,
+                                                           a.status);
+        }
+    }
+    static void gsym_tiles(const LaunchArgs &a, cudaStream_t st) {
+        switch (a.minb_s) {
+        case 12: gsym_v<12>(a, st); break;
+        case 16: gsym_v<16>(a, st); break;
+        default: gsym_v<8>(a, st); break;
+        }
+    }
+    static void gsym_reduce(const LaunchArgs &a, cudaStream_t st) {
+        if constexpr (Part<N>::size <= 32) {
+            constexpr int PS = Part<N>::size;
+            gsym_sum_kernel<N><<<(PS * a.K + 255) / 256, 256, 0, st>>>(
+                a.stile_start, a.LC_s, a.K, a.psym, a.psym + (size_t)a.nstiles * PS * 32, a.part);
+            grad_reduce_kernel<N><<<(a.K + 127) / 128, 128, 0, st>>>(a.part, a.K, a.bra, a.C, a.scal, a.g,
+                                                                      a.status);
+        }
     }
     static void matel(const LaunchArgs &a, const int *terms, int nterms, double *out,
                       cudaStream_t st) {
@@ -396,6 +546,16 @@ int launch_grad_reduce(const LaunchArgs &a, cudaStream_t st) {
 int launch_grad(const LaunchArgs &a, cudaStream_t st) {
     if (launch_grad_tiles(a, st)) return -1;
     return launch_grad_reduce(a, st);
+}
+int launch_gsym(const LaunchArgs &a, cudaStream_t st) {
+    if (a.n > 5) return -1;
+    NECG_DISPATCH(a.n, gsym_tiles(a, st));
+    return 0;
+}
+int launch_gsym_reduce(const LaunchArgs &a, cudaStream_t st) {
+    if (a.n > 5) return -1;
+    NECG_DISPATCH(a.n, gsym_reduce(a, st));
+    return 0;
 }
 int launch_matel(const LaunchArgs &a, const int *terms, int nterms, double *out, cudaStream_t st) {
     NECG_DISPATCH(a.n, matel(a, terms, nterms, out, st));

@@ -2,6 +2,8 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include "necg_lanes.cuh"
+
 namespace necg {
 
 struct LaunchArgs {
@@ -18,11 +20,20 @@ struct LaunchArgs {
     double *rows, *scal, *part, *g;        // device workspace / outputs
     double lam, scale_override;
     int *status;
+    // symmetric gradient pass
+    const int *pinv;                       // index of P^-1 per symmetry term (null: none)
+    KetMap kmap;                           // ket frame map per (P, field)
+    const int2 *stiles;                    // lower-triangle tiles of chunk LC_s
+    const int *stile_start;                // first tile of each 32-row block (nkb + 1)
+    int nstiles, LC_s, minb_s;
+    double *psym;                          // bra partials, then ket partials
 };
 
 int launch_prep(const LaunchArgs &a, cudaStream_t st);
 int launch_energy(const LaunchArgs &a, cudaStream_t st);
 int launch_grad(const LaunchArgs &a, cudaStream_t st);
+int launch_gsym(const LaunchArgs &a, cudaStream_t st);
+int launch_gsym_reduce(const LaunchArgs &a, cudaStream_t st);
 int launch_grad_tiles(const LaunchArgs &a, cudaStream_t st);
 int launch_grad_reduce(const LaunchArgs &a, cudaStream_t st);
 int launch_matel(const LaunchArgs &a, const int *terms, int nterms, double *out, cudaStream_t st);

@@ -100,7 +100,7 @@ NECG_HD void prep_bra_one(const double *iv, int K, const Consts<N> &cs, double *
 template <int N>
 NECG_HD void prep_ket_one(const double *iv, const double *C, int nst, const Consts<N> &cs,
                           const double *sml, const double *sms, const double *scvv, double *ket,
-                          int id) {
+                          int id, const int *pinv = nullptr) {
     using KL = KetLayout<N>;
     constexpr int blk = tri(N) + 3 * N;
     const int l = id / nst, P = id - l * nst;
@@ -163,7 +163,8 @@ NECG_HD void prep_ket_one(const double *iv, const double *C, int nst, const Cons
     o[KL::tMA] = tMA;
     o[KL::w] = scvv[P];
     o[KL::wC] = C ? 2.0 * scvv[P] * C[l] : 0.0;
-    if (KL::size > KL::wC + 1) o[KL::wC + 1] = 0.0;
+    o[KL::winv] = pinv ? scvv[pinv[P]] : 0.0;
+    if (KL::size > KL::winv + 1) o[KL::winv + 1] = 0.0;
 }
 
 // Energy tile lane: bra k against kets l in [l0, lend) (lend <= k + 1), all P.
@@ -221,28 +222,31 @@ template <int N> struct Part {
 
 // Gradient tile lane: bra k against kets l in [l0, l1), all P, weights
 // wC(l, P) = 2 scvv[P] C_l; writes the partial to part[f * stride] (f < Part::size).
-template <int N, typename R, typename BA, typename KB>
+template <int N, typename R, typename BA, typename KB, typename ACC>
 NECG_HD bool grad_lane(const BA &b, const KB &ket, int l0, int l1, int nst, const Consts<N> &cs,
-                       R lam, R E, double *part, size_t stride) {
+                       R lam, R E, double *part, size_t stride, ACC &acc) {
     using KL = KetLayout<N>;
     using PL = Part<N>;
-    R accG[tri(N)], accS[3 * N], accD = R(0.0);
-#pragma unroll
-    for (int t = 0; t < tri(N); ++t) accG[t] = R(0.0);
-#pragma unroll
-    for (int t = 0; t < 3 * N; ++t) accS[t] = R(0.0);
+    acc.zero();
     bool ok = true;
     for (int l = l0; l < l1; ++l)
         for (int P = 0; P < nst; ++P) {
             const auto kr = ket.at(((size_t)l * nst + P) * KL::size);
-            ok = term_grad<N>(b, kr, cs, lam, E, R(kr[KL::wC]), accG, accD, accS) && ok;
+            ok = term_grad<N>(b, kr, cs, lam, E, R(kr[KL::wC]), acc) && ok;
         }
 #pragma unroll
-    for (int t = 0; t < tri(N); ++t) part[(PL::G + t) * stride] = val(accG[t]);
-    part[PL::D * stride] = val(accD);
+    for (int t = 0; t < tri(N); ++t) part[(PL::G + t) * stride] = val(acc.g(t));
+    part[PL::D * stride] = val(acc.d());
 #pragma unroll
-    for (int t = 0; t < 3 * N; ++t) part[(PL::S + t) * stride] = val(accS[t]);
+    for (int t = 0; t < 3 * N; ++t) part[(PL::S + t) * stride] = val(acc.s(t));
     return ok;
+}
+
+template <int N, typename R, typename BA, typename KB>
+NECG_HD bool grad_lane(const BA &b, const KB &ket, int l0, int l1, int nst, const Consts<N> &cs,
+                       R lam, R E, double *part, size_t stride) {
+    RegAcc<N, R> acc;
+    return grad_lane<N, R>(b, ket, l0, l1, nst, cs, lam, E, part, stride, acc);
 }
 
 // Map an A-space gradient dF/dA = G + D A^-1 (G packed symmetric, D the
@@ -322,20 +326,16 @@ NECG_HD bool gradel_one(const BA &b, const KR &kr, const Consts<N> &cs, const do
     bool ok = true;
 #pragma unroll
     for (int which = 0; which < 2; ++which) {
-        R accG[tri(N)], accS[3 * N], accD = R(0.0);
-#pragma unroll
-        for (int q = 0; q < tri(N); ++q) accG[q] = R(0.0);
-#pragma unroll
-        for (int q = 0; q < 3 * N; ++q) accS[q] = R(0.0);
+        RegAcc<N, R> acc;
+        acc.zero();
         // which 0: dH (lam 1, E 0); which 1: dS (lam 0, E -1)
-        ok = term_grad<N>(b, kr, cs, R(which == 0 ? 1.0 : 0.0), R(which == 0 ? 0.0 : -1.0), R(1.0),
-                          accG, accD, accS) && ok;
+        ok = term_grad<N>(b, kr, cs, R(which == 0 ? 1.0 : 0.0), R(which == 0 ? 0.0 : -1.0), R(1.0), acc) && ok;
         double G[tri(N)], gS[3 * N];
 #pragma unroll
-        for (int q = 0; q < tri(N); ++q) G[q] = val(accG[q]);
+        for (int q = 0; q < tri(N); ++q) G[q] = val(acc.g(q));
 #pragma unroll
-        for (int q = 0; q < 3 * N; ++q) gS[q] = val(accS[q]);
-        a_to_vech<N>(G, val(accD), gS, L, diag ? 2.0 : 1.0, which == 0 ? tgvl : tgvls);
+        for (int q = 0; q < 3 * N; ++q) gS[q] = val(acc.s(q));
+        a_to_vech<N>(G, val(acc.d()), gS, L, diag ? 2.0 : 1.0, which == 0 ? tgvl : tgvls);
     }
     return ok;
 }
@@ -351,6 +351,24 @@ NECG_HD int energy_tile_count(int K, int LC) {
         n += last / LC + 1;
     }
     return n;
+}
+
+// Sparse linear map taking a ket gradient from P's transformed frame to the
+// basis function's own frame: dF/dA_l = sml dF/dA_l' sml^T (packed), the A^-1
+// coefficient unchanged, dF/ds_l = sms^T dF/ds_l'.  Entry (P, f): cnt values
+// at src/coef[(P * PS + f) * maxnz + i].
+struct KetMap {
+    const int *cnt, *src;
+    const double *coef;
+    int maxnz;
+};
+
+NECG_HD double ket_map_apply(const KetMap &m, int P, int f, int PS, const double *in) {
+    const int e = P * PS + f;
+    const int n = m.cnt[e];
+    double v = 0.0;
+    for (int i = 0; i < n; ++i) v += m.coef[(size_t)e * m.maxnz + i] * in[m.src[(size_t)e * m.maxnz + i]];
+    return v;
 }
 
 // Lane ranges of the two tile kinds (used by the kernels and the emulator).

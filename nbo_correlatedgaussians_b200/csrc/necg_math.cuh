@@ -72,7 +72,7 @@ __host__ __device__ constexpr int sx(int i, int j) {
 #define NECG_SQRT_PI 1.7724538509055159
 
 // Ket record: one per (l, P), read warp-uniformly by the tile kernels.
-// Layout (doubles): Ap[tri] Sp[3N] ASp[3N] Np[tri] AMp[N*N] i2 pre tMA w wC pad
+// Layout (doubles): Ap[tri] Sp[3N] ASp[3N] Np[tri] AMp[N*N] i2 pre tMA w wC winv pad
 template <int N> struct KetLayout {
     static constexpr int T = tri(N);
     static constexpr int Ap = 0;
@@ -85,7 +85,8 @@ template <int N> struct KetLayout {
     static constexpr int tMA = pre + 1;  // tr(M A_l')
     static constexpr int w = tMA + 1;    // symmetry weight scvv[P]
     static constexpr int wC = w + 1;     // 2 scvv[P] C_l (gradient weight)
-    static constexpr int size = (wC + 1 + 1) & ~1;  // even, 16-byte records
+    static constexpr int winv = wC + 1;  // scvv[P^-1] (ket weight of the symmetric pass)
+    static constexpr int size = (winv + 1 + 1) & ~1;  // even, 16-byte records
 };
 
 // Bra record: structure of arrays over k, field f of basis k at f*K + k.
@@ -132,6 +133,21 @@ struct BraRef {
     __device__ __forceinline__ double operator()(int f) const { return ldv(p + (size_t)f * K); }
 };
 #endif
+
+// Register accumulators of one bra gradient (see term_grad).
+template <int N, typename R> struct RegAcc {
+    R G[tri(N)], D, S[3 * N];
+    NECG_HD void zero() {
+#pragma unroll
+        for (int t = 0; t < tri(N); ++t) G[t] = R(0.0);
+        D = R(0.0);
+#pragma unroll
+        for (int t = 0; t < 3 * N; ++t) S[t] = R(0.0);
+    }
+    NECG_HD R &g(int t) { return G[t]; }
+    NECG_HD R &d() { return D; }
+    NECG_HD R &s(int t) { return S[t]; }
+};
 
 // ---------------------------------------------------------------------------
 // Cholesky of a packed SPD matrix B = R R^T; returns the inverse Bi (packed),
@@ -239,6 +255,76 @@ NECG_HD void boys(R a, R bb, R &fs, R &dfs, R &ia, R &z) {
         fs = (0.5 * NECG_SQRT_PI) * rb;
         if (GRAD) dfs = -0.5 * fs * a * rb * rb;  // F0' = -F0 / (2 z)
         else dfs = R(0.0);
+    }
+}
+
+// Coulomb sum with the pieces of its derivative (python/gradel.py:266-337):
+// rho = sum_v c_v F0(z_v) a_v^-1/2, Z' = sum_v alpha_v v b_v^T - (efs/2) q e_z^T
+// (the Stark part folded in), W = sum_v beta_v v v^T (packed).
+#pragma nv_exec_check_disable
+template <int N, typename R>
+NECG_HD void coulomb_grad(const R (&Bi)[tri(N)], const R (&T)[3 * N], const Consts<N> &cs, R &rho,
+                          R (&Z)[3 * N], R (&W)[tri(N)]) {
+#pragma unroll
+    for (int t = 0; t < 3 * N; ++t) Z[t] = R(0.0);
+#pragma unroll
+    for (int t = 0; t < tri(N); ++t) W[t] = R(0.0);
+    rho = R(0.0);
+#pragma unroll
+    for (int q = 1; q <= N; ++q)
+#pragma unroll
+        for (int p = 0; p < q; ++p) {
+            R a = Bi[sx(q - 1, q - 1)];
+            R bv[3];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) bv[c] = T[3 * (q - 1) + c];
+            if (p > 0) {
+                a += Bi[sx(p - 1, p - 1)] - 2.0 * Bi[sx(q - 1, p - 1)];
+#pragma unroll
+                for (int c = 0; c < 3; ++c) bv[c] -= T[3 * (p - 1) + c];
+            }
+            const R bb = bv[0] * bv[0] + bv[1] * bv[1] + bv[2] * bv[2];
+            R fs, dfs, ia, z;
+            boys<true>(a, bb, fs, dfs, ia, z);
+            const double c = cs.cv[vidx(p, q)];
+            rho += c * fs;
+            const R al = c * dfs * ia;
+            const R be = c * ia * (dfs * z + 0.5 * fs);
+#pragma unroll
+            for (int cc = 0; cc < 3; ++cc) Z[3 * (q - 1) + cc] += al * bv[cc];
+            W[sx(q - 1, q - 1)] += be;
+            if (p > 0) {
+#pragma unroll
+                for (int cc = 0; cc < 3; ++cc) Z[3 * (p - 1) + cc] -= al * bv[cc];
+                W[sx(p - 1, p - 1)] += be;
+                W[sx(q - 1, p - 1)] -= be;
+            }
+        }
+#pragma unroll
+    for (int i = 0; i < N; ++i) Z[3 * i + 2] -= 0.5 * cs.efs * cs.q[i];
+}
+
+// acc += Bi Mt Bi (Mt packed symmetric), column by column of Mt Bi.
+#pragma nv_exec_check_disable
+template <int N, typename R, typename OUT>
+NECG_HD void sandwich(const R (&Bi)[tri(N)], const R (&Mt)[tri(N)], OUT &&add) {
+#pragma unroll
+    for (int j = 0; j < N; ++j) {
+        R col[N];
+#pragma unroll
+        for (int a = 0; a < N; ++a) {
+            R s = Mt[sx(a, 0)] * Bi[sx(0, j)];
+#pragma unroll
+            for (int k = 1; k < N; ++k) s += Mt[sx(a, k)] * Bi[sx(k, j)];
+            col[a] = s;
+        }
+#pragma unroll
+        for (int i = j; i < N; ++i) {
+            R s = Bi[sx(i, 0)] * col[0];
+#pragma unroll
+            for (int a = 1; a < N; ++a) s += Bi[sx(i, a)] * col[a];
+            add(sx(i, j), s);
+        }
     }
 }
 
@@ -374,61 +460,24 @@ NECG_HD bool term_energy(const BA &b, const KA &kr, const Consts<N> &cs, R &ov, 
 // Full term with bra gradient.  Fw = wgt (lam h - E ov), ovw = wgt lam ov:
 // lam = 1, E = current energy gives the gradient of H - E S (the optimiser's
 // combination); lam = 1, E = 0 gives dH alone; lam = 0, E = -1 gives dS alone.
-// accG: packed dF/dA_k, accD: coefficient of A_k^-1 in dF/dA_k, accS: dF/ds_k (n x 3).
+// acc: accumulator with g(t) (packed dF/dA_k), d() (coefficient of A_k^-1 in
+// dF/dA_k) and s(t) (dF/ds_k, n x 3), each returning a reference -- registers
+// (RegAcc) or, on the device, lane-interleaved shared memory.
 #pragma nv_exec_check_disable
-template <int N, typename R, typename BA, typename KA>
-NECG_HD bool term_grad(const BA &b, const KA &kr, const Consts<N> &cs, R lam, R E, R wgt,
-                       R (&accG)[tri(N)], R &accD, R (&accS)[3 * N]) {
+template <int N, typename R, typename BA, typename KA, typename ACC>
+NECG_HD bool term_grad(const BA &b, const KA &kr, const Consts<N> &cs, R lam, R E, R wgt, ACC &acc) {
     using KL = KetLayout<N>;
     using BL = BraLayout<N>;
     R Bi[tri(N)], T[3 * N], ov;
     const bool ok = term_core<N>(b, kr, cs, Bi, T, ov);
     const R tau = term_tau<N>(b, kr, cs, Bi, T);
     const R sig = term_sig<N>(cs, T);
-    // Coulomb with derivatives: rho, Z (n x 3), W (packed)
-    R Z[3 * N], W[tri(N)];
-#pragma unroll
-    for (int t = 0; t < 3 * N; ++t) Z[t] = R(0.0);
-#pragma unroll
-    for (int t = 0; t < tri(N); ++t) W[t] = R(0.0);
-    R rho = R(0.0);
-#pragma unroll
-    for (int q = 1; q <= N; ++q)
-#pragma unroll
-        for (int p = 0; p < q; ++p) {
-            R a = Bi[sx(q - 1, q - 1)];
-            R bv[3];
-#pragma unroll
-            for (int c = 0; c < 3; ++c) bv[c] = T[3 * (q - 1) + c];
-            if (p > 0) {
-                a += Bi[sx(p - 1, p - 1)] - 2.0 * Bi[sx(q - 1, p - 1)];
-#pragma unroll
-                for (int c = 0; c < 3; ++c) bv[c] -= T[3 * (p - 1) + c];
-            }
-            const R bb = bv[0] * bv[0] + bv[1] * bv[1] + bv[2] * bv[2];
-            R fs, dfs, ia, z;
-            boys<true>(a, bb, fs, dfs, ia, z);
-            const double c = cs.cv[vidx(p, q)];
-            rho += c * fs;
-            const R al = c * dfs * ia;
-            const R be = c * ia * (dfs * z + 0.5 * fs);
-#pragma unroll
-            for (int cc = 0; cc < 3; ++cc) Z[3 * (q - 1) + cc] += al * bv[cc];
-            W[sx(q - 1, q - 1)] += be;
-            if (p > 0) {
-#pragma unroll
-                for (int cc = 0; cc < 3; ++cc) Z[3 * (p - 1) + cc] -= al * bv[cc];
-                W[sx(p - 1, p - 1)] += be;
-                W[sx(q - 1, p - 1)] -= be;
-            }
-        }
-    // Stark part of Z' (a per-problem constant column)
-#pragma unroll
-    for (int i = 0; i < N; ++i) Z[3 * i + 2] -= 0.5 * cs.efs * cs.q[i];
+    R Z[3 * N], W[tri(N)], rho;
+    coulomb_grad<N>(Bi, T, cs, rho, Z, W);
     const R h = ov * (2.0 * tau + rho - sig);
     const R Fw = wgt * (lam * h - E * ov);
     const R ovw = wgt * lam * ov;
-    accD += 0.75 * Fw;
+    acc.d() += 0.75 * Fw;
     // accG += Bi (ovw (6 N_l' + W) - 1.5 Fw B) Bi,  B = A_k + A_l'
     {
         const R f15 = 1.5 * Fw;
@@ -450,7 +499,7 @@ NECG_HD bool term_grad(const BA &b, const KA &kr, const Consts<N> &cs, R lam, R 
                 R s = Bi[sx(i, 0)] * col[0];
 #pragma unroll
                 for (int a = 1; a < N; ++a) s += Bi[sx(i, a)] * col[a];
-                accG[sx(i, j)] += s;
+                acc.g(sx(i, j)) += s;
             }
         }
     }
@@ -491,7 +540,7 @@ NECG_HD bool term_grad(const BA &b, const KA &kr, const Consts<N> &cs, R lam, R 
                 R s = b(BL::A + sx(i, 0)) * Q[c];
 #pragma unroll
                 for (int k = 1; k < N; ++k) s += b(BL::A + sx(i, k)) * Q[3 * k + c];
-                accS[3 * i + c] += o2 * s - f2 * Y[3 * i + c];
+                acc.s(3 * i + c) += o2 * s - f2 * Y[3 * i + c];
             }
     }
     // Rk = ovw Qk - Fw/2 Dk ; accG += Rk Dk^T + Dk Rk^T,  Dk = S_k - T
@@ -511,7 +560,146 @@ NECG_HD bool term_grad(const BA &b, const KA &kr, const Consts<N> &cs, R lam, R 
             R s = Q[3 * i] * T[3 * j] + T[3 * i] * Q[3 * j];
 #pragma unroll
             for (int c = 1; c < 3; ++c) s += Q[3 * i + c] * T[3 * j + c] + T[3 * i + c] * Q[3 * j + c];
-            accG[sx(i, j)] += s;
+            acc.g(sx(i, j)) += s;
+        }
+    return ok;
+}
+
+// Both gradients of one (k, l, P) term: the bra gradient (with respect to A_k,
+// s_k; weight wb) into acc, and the ket gradient with respect to the
+// transformed ket (A_l' = sml^T A_l sml, s_l' = sms s_l; weight wk) through
+// kout.put(f, value) / kout.add(f, value) for f in [0, tri(N) + 1 + 3N):
+// packed dF/dA_l', the coefficient of A_l'^-1, dF/ds_l'.  The element is symmetric under exchanging
+// bra and (transformed) ket, so the ket formulas are the bra formulas with the
+// roles swapped:
+//   dF/dA_l' = Fk (-Dl Dl^T - 1.5 Bi) + 0.75 Fk A_l'^-1
+//              + ovk (Bi (6 A_k M A_k + W) Bi - Ql Dl^T - Dl Ql^T)
+//   dF/ds_l' = 2 Fk Y + 2 ovk A_l' Ql,   Ql = Bi (Z' + 4 A_k M Y),  Dl = T - S_l'
+// with Fk = wk (h - E ov), ovk = wk ov.
+#pragma nv_exec_check_disable
+template <int N, typename R, typename BA, typename KA, typename ACC, typename KOUT>
+NECG_HD bool term_sym(const BA &b, const KA &kr, const Consts<N> &cs, R E, R wb, R wk, ACC &acc,
+                      KOUT &kout) {
+    using KL = KetLayout<N>;
+    using BL = BraLayout<N>;
+    R Bi[tri(N)], T[3 * N], ov;
+    const bool ok = term_core<N>(b, kr, cs, Bi, T, ov);
+    const R tau = term_tau<N>(b, kr, cs, Bi, T);
+    const R sig = term_sig<N>(cs, T);
+    R Z[3 * N], W[tri(N)], rho;
+    coulomb_grad<N>(Bi, T, cs, rho, Z, W);
+    const R phi = ov * (2.0 * tau + rho - sig) - E * ov;
+    const R Fb = wb * phi, ovb = wb * ov;
+    const R Fk = wk * phi, ovk = wk * ov;
+    acc.d() += 0.75 * Fb;
+    kout.put(tri(N), 0.75 * Fk);
+    // bra: acc += Bi (ovb (6 N_l' + W) - 1.5 Fb B) Bi ; ket: Bi (ovk (6 N_k + W) - 1.5 Fk B) Bi
+    {
+        R Mt[tri(N)];
+        const R fb = 1.5 * Fb, fk = 1.5 * Fk;
+#pragma unroll
+        for (int t = 0; t < tri(N); ++t)
+            Mt[t] = ovb * (6.0 * kr[KL::Np + t] + W[t]) - fb * (b(BL::A + t) + kr[KL::Ap + t]);
+        sandwich<N>(Bi, Mt, [&](int t, R v) { acc.g(t) += v; });
+#pragma unroll
+        for (int t = 0; t < tri(N); ++t)
+            W[t] = ovk * (6.0 * b(BL::Nk + t) + W[t]) - fk * (b(BL::A + t) + kr[KL::Ap + t]);
+        sandwich<N>(Bi, W, [&](int t, R v) { kout.put(t, v); });
+    }
+    // Y = A_l' (T - S_l'), MY = M Y
+    R Dl[3 * N], Y[3 * N];
+#pragma unroll
+    for (int t = 0; t < 3 * N; ++t) Dl[t] = T[t] - kr[KL::Sp + t];
+    symv3<N>(kr, KL::Ap, Dl, Y);
+    R Zl[3 * N];
+    {
+        R MY[3 * N];
+#pragma unroll
+        for (int i = 0; i < N; ++i)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                R s = cs.M[i * N] * Y[c];
+#pragma unroll
+                for (int k = 1; k < N; ++k) s += cs.M[i * N + k] * Y[3 * k + c];
+                MY[3 * i + c] = s;
+            }
+        // Zl = Z' + 4 A_k (M Y) ; Z <- Zk = Z' - 4 (A_l' M) Y
+#pragma unroll
+        for (int i = 0; i < N; ++i)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                R s = b(BL::A + sx(i, 0)) * MY[c];
+#pragma unroll
+                for (int k = 1; k < N; ++k) s += b(BL::A + sx(i, k)) * MY[3 * k + c];
+                Zl[3 * i + c] = Z[3 * i + c] + 4.0 * s;
+            }
+#pragma unroll
+        for (int i = 0; i < N; ++i)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                R s = kr[KL::AMp + i * N] * Y[c];
+#pragma unroll
+                for (int k = 1; k < N; ++k) s += kr[KL::AMp + i * N + k] * Y[3 * k + c];
+                Z[3 * i + c] -= 4.0 * s;
+            }
+    }
+    R Qk[3 * N], Ql[3 * N];
+#pragma unroll
+    for (int i = 0; i < N; ++i)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            R s = Bi[sx(i, 0)] * Z[c], t = Bi[sx(i, 0)] * Zl[c];
+#pragma unroll
+            for (int k = 1; k < N; ++k) {
+                s += Bi[sx(i, k)] * Z[3 * k + c];
+                t += Bi[sx(i, k)] * Zl[3 * k + c];
+            }
+            Qk[3 * i + c] = s;
+            Ql[3 * i + c] = t;
+        }
+    // bra: acc.s += 2 ovb A_k Qk - 2 Fb Y ; ket: put 2 ovk A_l' Ql + 2 Fk Y
+    {
+        const R ob2 = 2.0 * ovb, fb2 = 2.0 * Fb, ok2 = 2.0 * ovk, fk2 = 2.0 * Fk;
+#pragma unroll
+        for (int i = 0; i < N; ++i)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                R s = b(BL::A + sx(i, 0)) * Qk[c];
+                R t = kr[KL::Ap + sx(i, 0)] * Ql[c];
+#pragma unroll
+                for (int k = 1; k < N; ++k) {
+                    s += b(BL::A + sx(i, k)) * Qk[3 * k + c];
+                    t += kr[KL::Ap + sx(i, k)] * Ql[3 * k + c];
+                }
+                acc.s(3 * i + c) += ob2 * s - fb2 * Y[3 * i + c];
+                kout.put(tri(N) + 1 + 3 * i + c, ok2 * t + fk2 * Y[3 * i + c]);
+            }
+    }
+    // bra: Rk = ovb Qk - Fb/2 Dk, acc.g += Rk Dk^T + Dk Rk^T   (Dk = S_k - T)
+    // ket: Rl = ovk Ql + Fk/2 Dl, dF/dA_l' -= Rl Dl^T + Dl Rl^T
+    {
+        const R fbh = 0.5 * Fb, fkh = 0.5 * Fk;
+#pragma unroll
+        for (int t = 0; t < 3 * N; ++t) {
+            const R dk = b(BL::S + t) - T[t];
+            T[t] = dk;
+            Qk[t] = ovb * Qk[t] - fbh * dk;
+            Ql[t] = ovk * Ql[t] + fkh * Dl[t];
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < N; ++i)
+#pragma unroll
+        for (int j = 0; j <= i; ++j) {
+            R s = Qk[3 * i] * T[3 * j] + T[3 * i] * Qk[3 * j];
+            R t = Ql[3 * i] * Dl[3 * j] + Dl[3 * i] * Ql[3 * j];
+#pragma unroll
+            for (int c = 1; c < 3; ++c) {
+                s += Qk[3 * i + c] * T[3 * j + c] + T[3 * i + c] * Qk[3 * j + c];
+                t += Ql[3 * i + c] * Dl[3 * j + c] + Dl[3 * i + c] * Ql[3 * j + c];
+            }
+            acc.g(sx(i, j)) += s;
+            kout.add(sx(i, j), -t);
         }
     return ok;
 }

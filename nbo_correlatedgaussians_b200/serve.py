@@ -39,12 +39,15 @@ def workspace_estimate(p: Problem, K_max: int | None = None) -> int:
     """Device bytes a run's Engine allocates (mirror of necg_create's sizes)."""
     K, n, nst = int(K_max or p.K), p.n, p.nst
     tri = n * (n + 1) // 2
-    ket = (tri + 6 * n + tri + n * n + 5 + 1) & ~1
+    ket = (2 * tri + 6 * n + n * n + 5 + 2) & ~1
     bra = tri + 6 * n + tri + 3 + tri
     ps = tri + 1 + 3 * n
     blk = tri + 3 * n
+    # symmetric-pass partials at its narrowest ket chunk (2)
+    ntiles = sum(min(kb * 32 + 31, K - 1) // 2 + 1 for kb in range((K + 31) // 32))
+    sym = ntiles * ps * (32 + 2) if n <= 5 else 0
     doubles = (bra * K + ket * K * nst + ps * K * ((K + 3) // 4) + 2 * K * K + 2 * K + 4
-               + 2 * (K * blk + K) + 2 + nst * (n * n + 9 * n * n + 1))
+               + 2 * (K * blk + K) + 2 + nst * (n * n + 9 * n * n + 1) + sym)
     return 8 * doubles + 3 * 8 * (K * blk + K) + 4096
 
 

@@ -7,6 +7,7 @@
 #include <math.h>
 #include <string.h>
 
+#include <algorithm>
 #include <vector>
 
 #include "../../nbo_correlatedgaussians_b200/csrc/necg_hostscalar.cuh"
@@ -99,6 +100,184 @@ int outprod(const Args &a, const double *x, int LCe, int LCg, double *f, double 
     return flags;
 }
 
+// Host mirror of the symmetric gradient pass (gsym_kernel + gsym_sum_kernel):
+// same tiles, same per-lane term_sym, the warp's column sums taken in lane
+// order, the same ket-frame map.
+struct HostMap {
+    std::vector<int> cnt, src;
+    std::vector<double> coef;
+    int maxnz = 1;
+    std::vector<int> pinv;
+    bool ok = false;
+};
+
+template <int N> HostMap build_map(const Args &a) {
+    HostMap hm;
+    const int n = N, nst = a.nst, m = 3 * n, T = tri(N), PS = T + 1 + m;
+    hm.pinv.assign(nst, -1);
+    for (int p = 0; p < nst; ++p)
+        for (int q = 0; q < nst && hm.pinv[p] < 0; ++q) {
+            bool ok = true;
+            for (int i = 0; i < n && ok; ++i)
+                for (int j = 0; j < n && ok; ++j) {
+                    double s = 0.0;
+                    for (int k = 0; k < n; ++k) s += a.sml[p * n * n + i * n + k] * a.sml[q * n * n + k * n + j];
+                    ok = fabs(s - (i == j)) < 1e-12;
+                }
+            for (int i = 0; i < m && ok; ++i)
+                for (int j = 0; j < m && ok; ++j) {
+                    double s = 0.0;
+                    for (int k = 0; k < m; ++k) s += a.sms[p * m * m + i * m + k] * a.sms[q * m * m + k * m + j];
+                    ok = fabs(s - (i == j)) < 1e-12;
+                }
+            if (ok) hm.pinv[p] = q;
+        }
+    for (int p = 0; p < nst; ++p)
+        if (hm.pinv[p] < 0) return hm;
+    std::vector<std::vector<std::pair<int, double>>> rows((size_t)nst * PS);
+    for (int p = 0; p < nst; ++p) {
+        const double *P = a.sml + (size_t)p * n * n, *Sm = a.sms + (size_t)p * m * m;
+        for (int x = 0; x < n; ++x)
+            for (int y = 0; y <= x; ++y) {
+                std::vector<double> c(T, 0.0);
+                for (int u = 0; u < n; ++u)
+                    for (int v = 0; v < n; ++v) c[sx(u, v)] += P[x * n + u] * P[y * n + v];
+                for (int s2 = 0; s2 < T; ++s2)
+                    if (c[s2] != 0.0) rows[(size_t)p * PS + sx(x, y)].push_back({s2, c[s2]});
+            }
+        rows[(size_t)p * PS + T].push_back({T, 1.0});
+        for (int r = 0; r < m; ++r)
+            for (int u = 0; u < m; ++u)
+                if (Sm[u * m + r] != 0.0) rows[(size_t)p * PS + T + 1 + r].push_back({T + 1 + u, Sm[u * m + r]});
+    }
+    for (auto &r : rows) hm.maxnz = (int)r.size() > hm.maxnz ? (int)r.size() : hm.maxnz;
+    hm.cnt.resize(rows.size());
+    hm.src.assign(rows.size() * hm.maxnz, 0);
+    hm.coef.assign(rows.size() * hm.maxnz, 0.0);
+    for (size_t e = 0; e < rows.size(); ++e) {
+        hm.cnt[e] = (int)rows[e].size();
+        for (size_t i = 0; i < rows[e].size(); ++i) {
+            hm.src[e * hm.maxnz + i] = rows[e][i].first;
+            hm.coef[e * hm.maxnz + i] = rows[e][i].second;
+        }
+    }
+    hm.ok = true;
+    return hm;
+}
+
+struct RowOutH {
+    double *r;
+    void put(int f, CD v) { r[f] = v.v; }
+    void add(int f, CD v) { r[f] += v.v; }
+};
+
+template <int N> int outprod_sym(const Args &a, const double *x, int LCe, int LCs, double *f, double *g, double *H,
+                                 double *S) {
+    const int K = a.K, nst = a.nst;
+    constexpr int PS = Part<N>::size;
+    if (PS > 32) return -2;
+    const size_t siv = (size_t)K * (tri(N) + 3 * N);
+    const double *iv = x, *C = x + siv;
+    HostMap hm = build_map<N>(a);
+    if (!hm.ok) return -3;
+    Consts<N> cs = consts<N>(a.mass, a.ncv, a.efs);
+    std::vector<double> bra((size_t)BraLayout<N>::size * K), ket((size_t)KetLayout<N>::size * K * nst);
+    for (int k = 0; k < K; ++k) prep_bra_one<N>(iv, K, cs, bra.data(), k);
+    for (int id = 0; id < K * nst; ++id)
+        prep_ket_one<N>(iv, C, nst, cs, a.sml, a.sms, a.scvv, ket.data(), id, hm.pinv.data());
+    int flags = 0;
+    for (int kb = 0; kb * 32 < K; ++kb)
+        for (int lc = 0; lc * LCe <= kb * 32 + 31 && lc * LCe < K; ++lc)
+            for (int lane = 0; lane < 32; ++lane) {
+                int k, l0, lend, bad = 0;
+                if (!energy_lane_range(kb, lc, lane, LCe, K, k, l0, lend)) continue;
+                flags |= energy_lane<N, CD>(HostBra{bra.data() + k, (size_t)K}, HostKetBase{ket.data()}, k, l0,
+                                            lend, K, nst, cs, H, S, nullptr, nullptr, bad);
+            }
+    std::vector<double> rh(K), rs(K);
+    double cHc = 0.0, cSc = 0.0;
+    for (int i = 0; i < K; ++i) {
+        double hh = 0.0, ss = 0.0;
+        for (int j = 0; j < K; ++j) {
+            hh += H[(size_t)i * K + j] * C[j];
+            ss += S[(size_t)i * K + j] * C[j];
+        }
+        rh[i] = hh;
+        rs[i] = ss;
+        cHc += C[i] * hh;
+        cSc += C[i] * ss;
+    }
+    const double E = cHc / cSc, norm = 1.0 / cSc;
+    *f = E;
+    for (int i = 0; i < K; ++i) g[siv + i] = 2.0 * norm * (rh[i] - E * rs[i]);
+    // symmetric tiles
+    std::vector<int> tstart;
+    std::vector<std::pair<int, int>> tiles;
+    for (int kb = 0; kb * 32 < K; ++kb) {
+        tstart.push_back((int)tiles.size());
+        const int last = kb * 32 + 31 < K - 1 ? kb * 32 + 31 : K - 1;
+        for (int lc = 0; lc <= last / LCs; ++lc) tiles.push_back({kb, lc});
+    }
+    tstart.push_back((int)tiles.size());
+    const int nt = (int)tiles.size();
+    std::vector<double> pb((size_t)nt * PS * 32, 0.0), pk((size_t)nt * LCs * PS, 0.0);
+    KetMap km{hm.cnt.data(), hm.src.data(), hm.coef.data(), hm.maxnz};
+    for (int t = 0; t < nt; ++t) {
+        const int kb = tiles[t].first, l0 = tiles[t].second * LCs, l1 = std::min(l0 + LCs, K);
+        std::vector<RegAcc<N, CD>> accs(32);
+        for (auto &ac : accs) ac.zero();
+        for (int l = l0; l < l1; ++l) {
+            double accl[32] = {0.0};
+            for (int P = 0; P < nst; ++P) {
+                const double *krp = ket.data() + ((size_t)l * nst + P) * KetLayout<N>::size;
+                double rows[32][33];
+                for (int lane = 0; lane < 32; ++lane) {
+                    const int k = kb * 32 + lane;
+                    for (int ff = 0; ff < PS; ++ff) rows[lane][ff] = 0.0;
+                    if (k < K && l <= k) {
+                        const double wk = l < k ? 2.0 * C[k] * krp[KetLayout<N>::winv] : 0.0;
+                        RowOutH ro{rows[lane]};
+                        if (!term_sym<N, CD>(HostBra{bra.data() + k, (size_t)K}, HostKet{krp}, cs, CD(E),
+                                             CD(krp[KetLayout<N>::wC]), CD(wk), accs[lane], ro))
+                            flags |= 1;
+                    }
+                }
+                double red[32];
+                for (int j = 0; j < 32; ++j) {
+                    double v = 0.0;
+                    if (j < PS)
+                        for (int r = 0; r < 32; ++r) v += rows[r][j];
+                    red[j] = v;
+                }
+                for (int j = 0; j < PS; ++j) accl[j] += ket_map_apply(km, P, j, PS, red);
+            }
+            for (int j = 0; j < PS; ++j) pk[((size_t)t * LCs + (l - l0)) * PS + j] = accl[j];
+        }
+        for (int lane = 0; lane < 32; ++lane) {
+            if (kb * 32 + lane >= K) continue;
+            for (int tt = 0; tt < tri(N); ++tt) pb[((size_t)t * PS + tt) * 32 + lane] = accs[lane].g(tt).v;
+            pb[((size_t)t * PS + tri(N)) * 32 + lane] = accs[lane].d().v;
+            for (int tt = 0; tt < 3 * N; ++tt) pb[((size_t)t * PS + tri(N) + 1 + tt) * 32 + lane] = accs[lane].s(tt).v;
+        }
+    }
+    std::vector<double> out((size_t)PS * K, 0.0);
+    const int nkb = (K + 31) / 32;
+    for (int ff = 0; ff < PS; ++ff)
+        for (int m = 0; m < K; ++m) {
+            const int kb = m / 32, lane = m % 32;
+            double s = 0.0;
+            for (int t = tstart[kb]; t < tstart[kb + 1]; ++t) s += pb[((size_t)t * PS + ff) * 32 + lane];
+            const int lc = m / LCs, ll = m % LCs;
+            int kb0 = lc * LCs - 31;
+            kb0 = kb0 > 0 ? (kb0 + 31) / 32 : 0;
+            for (int q = kb0; q < nkb; ++q) s += pk[((size_t)(tstart[q] + lc) * LCs + ll) * PS + ff];
+            out[(size_t)ff * K + m] = s;
+        }
+    for (int k = 0; k < K; ++k)
+        if (!grad_reduce_one<N>(out.data(), 1, K, bra.data(), norm * C[k], g, k)) flags |= 2;
+    return flags;
+}
+
 template <int N>
 int elements(const Args &a, const double *iv, int nterms, const int *terms, double *mat,
              double *tg, double *tgs) {
@@ -138,6 +317,13 @@ extern "C" int emu_outprod(int n, int nst, int K, double efs, const double *mass
                            int lc_e, int lc_g, double *f, double *g, double *H, double *S) {
     Args a{nst, K, efs, mass, ncv, scvv, sml, sms};
     EMU_DISPATCH(n, (outprod<N>(a, x, lc_e, lc_g, f, g, H, S)));
+}
+
+extern "C" int emu_outprod_sym(int n, int nst, int K, double efs, const double *mass, const double *ncv,
+                               const double *scvv, const double *sml, const double *sms, const double *x,
+                               int lc_e, int lc_s, double *f, double *g, double *H, double *S) {
+    Args a{nst, K, efs, mass, ncv, scvv, sml, sms};
+    EMU_DISPATCH(n, (outprod_sym<N>(a, x, lc_e, lc_s, f, g, H, S)));
 }
 
 extern "C" int emu_elements(int n, int nst, int K, double efs, const double *mass, const double *ncv,

@@ -65,3 +65,24 @@ def test_not_positive_definite_flag():
     p.iv[2 * p.blk:2 * p.blk + p.svh] = 0.0
     rc, f, g, H, S = emu.outprod(p)
     assert rc & 1
+
+
+@pytest.mark.parametrize("system,K,lc_s", [("He", 45, 1), ("He", 45, 6), ("H2", 37, 3), ("H2", 70, 8),
+                                           ("LiH", 33, 4), ("LiH", 40, 7)])
+def test_symmetric_pass_vs_oracle(system, K, lc_s):
+    """Unordered pairs with bra and ket gradients from one term, ket gradients
+    mapped back through each symmetry term's inverse frame."""
+    p = synth.make_problem(system, K, 11 * K)
+    p.C = np.random.default_rng(K + 1).normal(size=K)
+    fo, go = Oracle.from_problem(p).outprod(p.x, nthreads=8)
+    rc, f, g, H, S = emu.outprod_sym(p, 4, lc_s)
+    assert rc == 0
+    assert abs(f - fo) < TOL_E
+    assert normwise(g, go) < TOL_G
+
+
+def test_symmetric_pass_oldquit():
+    d = golden("oldquit.npz")
+    p = problem_from(d)
+    rc, f, g, H, S = emu.outprod_sym(p, 4, 4)
+    assert rc == 0 and abs(f - 4.296758204100342) < TOL_E and normwise(g, d["g"]) < TOL_G

@@ -195,3 +195,44 @@ def test_errors(torch_cuda):
     # the handle stays usable after the error
     f, g = eng.outprod(p.x)
     assert np.isfinite(f)
+
+
+@pytest.mark.parametrize("system,K", [("He", 80), ("H2", 90), ("LiH", 70)])
+def test_symmetric_and_ordered_gradient_passes_agree(torch_cuda, system, K):
+    """The unordered-pair gradient pass (bra and ket gradient per term) against
+    the ordered pass of the reference's loop structure and against the oracle."""
+    from nbo_correlatedgaussians_b200 import _lib, synth
+    p = synth.make_problem(system, K, 5 * K)
+    p.C = np.random.default_rng(K).normal(size=K)
+    eng = _engine(p)
+    L = eng.L
+    assert L.necg_set_symmetric(eng.h, 1, 4, 8) == _lib.NECG_OK
+    fs, gs = eng.outprod(p.x)
+    assert L.necg_set_symmetric(eng.h, 1, 7, 12) == _lib.NECG_OK
+    fs2, gs2 = eng.outprod(p.x)
+    assert L.necg_set_symmetric(eng.h, 0, 4, 8) == _lib.NECG_OK
+    fo, go = eng.outprod(p.x)
+    fr, gr = Oracle.from_problem(p).outprod(p.x, nthreads=8)
+    assert fs == fo == fs2  # the energy pass is shared
+    assert normwise(gs, gr) < TOL_G and normwise(gs2, gr) < TOL_G and normwise(go, gr) < TOL_G
+    assert normwise(gs, go) < 1e-12
+
+
+def test_symmetric_pass_unavailable_without_inverse_closure(torch_cuda):
+    from nbo_correlatedgaussians_b200 import _lib, synth
+    p = synth.make_problem("H2", 20, 4)
+    keep = [0, 2]  # identity and the proton swap: closed
+    q = p.copy()
+    q.sml, q.sms, q.scvv = p.sml[[0, 1]], p.sms[[0, 1]], p.scvv[[0, 1]]
+    assert _engine(q).L.necg_set_symmetric(_engine(q).h, 1, 4, 8) == _lib.NECG_OK
+    r = p.copy()  # a lone non-involutory map has no inverse in the set
+    M = np.array([[1.0, 0, 0], [0, 0, 1.0], [0, 1.0, 0]]) @ np.array([[1.0, 0, 0], [1.0, 1.0, 0], [0, 0, 1.0]])
+    r.sml = np.stack([np.eye(3), M])
+    r.sms = np.stack([np.eye(9), np.kron(np.linalg.inv(M), np.eye(3))])
+    r.scvv = np.array([0.5, 0.5])
+    e = _engine(r)
+    assert e.L.necg_set_symmetric(e.h, 1, 4, 8) == _lib.NECG_ERR_UNSUPPORTED
+    f, g = e.outprod(r.x)  # ordered pass still works
+    fo, go = Oracle.from_problem(r).outprod(r.x, nthreads=4)
+    assert abs(f - fo) < TOL_E and normwise(g, go) < TOL_G
+    del keep
