@@ -288,17 +288,30 @@ def run_engine(args):
 
     K, nst, n = prob.K, prob.nst, prob.n
     tf = term_flops(n)
-    grad_flops = K * K * nst * tf["grad"]
-    energy_flops = (K * (K + 1) // 2) * nst * tf["energy"]
+    mode = int(tiles.get("sym", 0))
+    unordered = (K * (K + 1) // 2) * nst
     ph = np.array(phases)
     ph_mean = ph.mean(axis=0)
-    grad_ms = float(ph_mean[3])
-    achieved = grad_flops / (grad_ms * 1e-3) / 1e12
+    energy_flops = unordered * tf["energy"]
+    if mode == 2:  # one pass over unordered pairs: H, S and both gradients
+        kname, per_term = f"fsym_kernel<{n}>", "fused"
+        kern_flops, kern_ms = unordered * tf["fused"], float(ph_mean[1])
+        eval_flops = kern_flops
+    elif mode == 1:  # energy pass + unordered pairs with bra and ket gradients
+        kname, per_term = f"gsym_kernel<{n}>", "sym"
+        kern_flops, kern_ms = unordered * tf["sym"], float(ph_mean[3])
+        eval_flops = kern_flops + energy_flops
+    else:  # energy pass + ordered pairs (the reference's loop structure)
+        kname, per_term = f"grad_kernel<{n}>", "grad"
+        kern_flops, kern_ms = K * K * nst * tf["grad"], float(ph_mean[3])
+        eval_flops = kern_flops + energy_flops
+    ordered_equiv = K * K * nst * tf["grad"] + energy_flops
+    achieved = kern_flops / (kern_ms * 1e-3) / 1e12
     traffic = None
     tpath = os.path.join(HERE, "profiles", "traffic.json")
     if os.path.exists(tpath):
         try:
-            traffic = json.load(open(tpath)).get(f"grad_kernel_{args.workload}")
+            traffic = json.load(open(tpath)).get(f"{kname}|{args.workload}")
         except (OSError, ValueError):
             traffic = None
     cpu = None
@@ -312,24 +325,32 @@ def run_engine(args):
         "config": {"workload": args.workload, "desc": WORKLOADS[args.workload],
                    "pair_elements_per_eval": prob.pairs, "terms_per_eval": (prob.pairs + K * K) * nst,
                    "l2": "flushed between steps by a 256 MiB write, not timed",
-                   "tiles": {k: tiles[k] for k in ("lc_e", "minb_e", "lc_g", "minb_g")},
+                   "pair_pass": ("fused energy + gradient, unordered pairs" if mode == 2 else
+                                 "energy pass + gradient over unordered pairs" if mode == 1 else
+                                 "energy pass + gradient over ordered pairs"),
+                   "tiles": {k: tiles[k] for k in ("lc_e", "minb_e", "lc_g", "minb_g", "sym", "lc_s", "minw_s")
+                             if k in tiles},
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
         "pair_elements_per_s": value * prob.pairs,
         "energy": E,
         "phase_ms": dict(zip(PHASES, [round(float(v), 4) for v in ph_mean])),
-        "roofline": {"bound": "fp64", "kernel": f"grad_kernel<{n}>", "achieved": achieved, "peak": peak.value,
+        "roofline": {"bound": "fp64", "kernel": kname, "achieved": achieved, "peak": peak.value,
                      "unit": "TFLOP/s", "frac": achieved / peak.value, "traffic": traffic,
                      "peak_source": "measured now by the FP64 FMA probe (necg_fp64_peak); "
                                     "MEASURED_PEAKS.json has no FP64 figure; nominal B200 FP64 = 37 TFLOP/s",
-                     "flops_per_launch": grad_flops, "flops_per_term": tf["grad"],
-                     "special_per_term": tf["grad_special"],
-                     "energy_kernel": {"achieved": energy_flops / (float(ph_mean[1]) * 1e-3) / 1e12,
-                                       "flops_per_launch": energy_flops},
-                     "whole_eval_tflops": (grad_flops + energy_flops) / (total_ms / args.steps * 1e-3) / 1e12},
+                     "flops_per_launch": kern_flops, "flops_per_term": tf[per_term],
+                     "special_per_term": tf[per_term + "_special"],
+                     "energy_kernel": (None if mode == 2 else
+                                       {"achieved": energy_flops / (float(ph_mean[1]) * 1e-3) / 1e12,
+                                        "flops_per_launch": energy_flops}),
+                     "whole_eval_tflops": eval_flops / (total_ms / args.steps * 1e-3) / 1e12,
+                     "reference_loop_equivalent_tflops": ordered_equiv / (total_ms / args.steps * 1e-3) / 1e12},
         "e2e": {"value": e2e_value, "unit": "evals/s", "h2d_bytes_per_step": int(prob.x.nbytes),
                 "d2h_bytes_per_step": int(prob.x.nbytes) + 8,
                 "path": "necg_outprod_host (pinned host x -> f, g)"},
-        "gpu_launches": (9 if (prob.K + tiles["lc_g"] - 1) // tiles["lc_g"] > 1 else 8) * args.steps,
+        # status reset, 2 prep, pair pass(es), rows + finalize, partial sum(s), reduce
+        "gpu_launches": (8 if mode == 2 else 9 if mode == 1 or (prob.K + tiles["lc_g"] - 1) // tiles["lc_g"] > 1
+                         else 8) * args.steps,
         "cpu_baseline": cpu,
         "clocks": clk,
     }

@@ -71,14 +71,17 @@ int necg_set_tiles(necg_handle *h, int lc_energy, int lc_grad);
  * shared memory instead of registers.  Set by the autotuner. */
 int necg_set_variant(necg_handle *h, int minw_energy, int minw_grad);
 
-/* Gradient pass over unordered pairs: each (k >= l, P) term yields the bra
- * gradient for k and the ket gradient for l, halving the terms of the ordered
- * pass (which follows python/make_grad.py:37-55 and evaluates every ordered
- * pair).  Needs a symmetry set closed under inverse (each sml and sms has its
- * inverse in the set) and n <= 5; otherwise NECG_ERR_UNSUPPORTED and the ordered
- * pass stays in use.  On by default when available.  lc: kets per tile (1..64);
- * minw: 8, 12 or 16 warps per SM.  Set by the autotuner. */
-int necg_set_symmetric(necg_handle *h, int enable, int lc, int minw);
+/* Choice of the pair pass.  mode 0: ordered pairs, the loop structure of
+ * python/make_grad.py:37-55 (every ordered pair, bra gradient only).  mode 1
+ * (default when available): each (k >= l, P) term yields the bra gradient for
+ * k and the ket gradient for l, halving the terms.  mode 2: as 1, fused with
+ * the energy pass -- one pass over unordered pairs writes H, S and the
+ * gradients of H and of S, combined once E is known (applies to necg_outprod;
+ * the gradient-only entry points use mode 1).  Modes 1 and 2 need a symmetry
+ * set closed under inverse (each sml and sms has its inverse in the set) and
+ * n <= 5; otherwise NECG_ERR_UNSUPPORTED.  lc: kets per tile (1..64); minw: 8,
+ * 12 or 16 warps per SM.  Set by the autotuner. */
+int necg_set_symmetric(necg_handle *h, int mode, int lc, int minw);
 
 /* One objective evaluation: python/outprod.py:20-76 outprod(x) -> (f, g),
  * including make_grad (python/make_grad.py:18-90).  Device pointers; H_dev and
@@ -211,8 +214,10 @@ int necg_fp64_peak(int iters, double *tflops, void *stream);
 const char *necg_status_string(int code);
 
 /* Algorithmic FP64 operation count of one (k, l, P) term (FMA = 2, add/mul = 1,
- * div/sqrt/rsqrt/exp = 1 each) for the energy kernel (which = 0) and the
- * gradient kernel (which = 1); *special receives the div/sqrt/exp part. */
+ * div/sqrt/rsqrt/exp = 1 each): which = 0 energy kernel, 1 ordered gradient
+ * kernel, 2 one unordered term of the symmetric gradient pass (bra and ket
+ * gradients), 3 one unordered term of the fused pass (H and S elements, bra
+ * and ket gradients of H and of S); *special receives the div/sqrt/exp part. */
 long long necg_term_flops(int n, int which, long long *special);
 
 #ifdef __cplusplus

@@ -15,7 +15,9 @@ The search space:
          these are the only distinct budgets)
   sym    gradient pass over unordered pairs (bra and ket gradient per term,
          when the symmetry set is closed under inverse) instead of ordered
-         pairs, with its own ket chunk lc_s and variant minw_s
+         pairs, with its own ket chunk lc_s and variant minw_s; sym = 2 fuses
+         it with the energy pass (one pass for H, S and both gradients), kept
+         when its total beats the best separate energy + gradient passes
 """
 from __future__ import annotations
 
@@ -37,6 +39,7 @@ MINB = (8, 12, 16, 20)
 MINB_GRAD_EXTRA = (112, 116)  # gradient kernel with shared-memory accumulators
 LC_S = (2, 4, 8, 16)          # kets per tile of the symmetric gradient pass
 MINW_SYM = (8, 12)
+MINW_FUSED = (8, 12, 16)
 
 
 def _bucket(K: int) -> int:
@@ -116,6 +119,20 @@ def tune(eng: Engine, x, K: int, reps: int = 3, report: bool = False) -> dict:
                 rows.append({"sym": 1, "minw": minw, "lc_s": lc, "grad_ms": g_ms})
                 if g_ms < res["grad_ms"]:
                     res.update(grad_ms=g_ms, sym=1, lc_s=lc, minw_s=minw)
+        # fused energy + symmetric gradient pass: phase 1 is the whole pair pass
+        best_sep = res["energy_ms"] + res["grad_ms"]
+        fused = None
+        for minw in MINW_FUSED:
+            for lc in LC_S:
+                _lib.check(L.necg_set_symmetric(eng.h, 2, lc, minw), "necg_set_symmetric")
+                _phase_times(eng, x, K, 1)
+                t = _phase_times(eng, x, K, reps).min(axis=0)
+                tot = float(t[1] + t[3] + t[4])
+                rows.append({"sym": 2, "minw": minw, "lc_s": lc, "total_ms": tot})
+                if tot < best_sep and (fused is None or tot < fused[0]):
+                    fused = (tot, lc, minw)
+        if fused is not None:
+            res.update(sym=2, lc_s=fused[1], minw_s=fused[2], fused_ms=fused[0])
     if report:
         res["table"] = rows
     apply(eng, res)

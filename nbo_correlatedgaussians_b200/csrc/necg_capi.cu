@@ -90,7 +90,11 @@ int ensure_tiles(necg_handle *h, int K, cudaStream_t st) {
 // Lower-triangle tiles of chunk LC for the symmetric pass, plus the first tile
 // of each 32-row block; the partial buffer grows here if this K and LC need more.
 int ensure_sym_tiles(necg_handle *h, int K, cudaStream_t st) {
-    if (h->stiles_K == K && h->stiles_lc == h->lc_s) return NECG_OK;
+    const int PS = necg::part_stride(h->n);
+    const size_t mult = h->grad_mode == 2 ? 2 : 1;  // the fused pass keeps H and S partials apart
+    if (h->stiles_K == K && h->stiles_lc == h->lc_s &&
+        (size_t)h->nstiles * PS * (32 + h->lc_s) * mult <= h->psym_cap)
+        return NECG_OK;
     std::vector<int2> t;
     std::vector<int> start;
     const int nkb = (K + 31) / 32, LC = h->lc_s;
@@ -107,8 +111,7 @@ int ensure_sym_tiles(necg_handle *h, int K, cudaStream_t st) {
         h->stiles_cap = (int)t.size();
     }
     if (!h->d_stile_start) CK(cudaMalloc((void **)&h->d_stile_start, ((h->K_max + 31) / 32 + 2) * sizeof(int)));
-    const int PS = necg::part_stride(h->n);
-    const size_t need = t.size() * (size_t)PS * (32 + LC);
+    const size_t need = t.size() * (size_t)PS * (32 + LC) * mult;
     if (need > h->psym_cap) {
         if (h->d_psym) cudaFree(h->d_psym);
         h->d_psym = nullptr;
@@ -195,7 +198,7 @@ int setup_symmetric(necg_handle *h) {
     CK(cudaMemcpy(h->d_kcoef, coef.data(), coef.size() * sizeof(double), cudaMemcpyHostToDevice));
     h->kmaxnz = maxnz;
     h->sym_ok = true;
-    h->use_sym = true;
+    h->grad_mode = 1;
     return NECG_OK;
 }
 
@@ -236,9 +239,11 @@ LaunchArgs base_args(necg_handle *h, int K) {
 }
 
 // The gradient passes after E and norm are in scal: symmetric (unordered pairs)
-// when available, ordered otherwise.
+// when available, ordered otherwise.  (Mode 2 fuses the symmetric pass with the
+// energy pass of necg_outprod; here H and S are already known, so the
+// symmetric pass alone is used.)
 int launch_gradient(necg_handle *h, LaunchArgs &a, cudaStream_t st) {
-    if (h->use_sym) {
+    if (h->grad_mode >= 1) {
         int rc = ensure_sym_tiles(h, a.K, st);
         if (rc) return rc;
         a.stiles = h->d_stiles;
@@ -355,10 +360,11 @@ int necg_set_tiles(necg_handle *h, int lc_energy, int lc_grad) {
     return NECG_OK;
 }
 
-int necg_set_symmetric(necg_handle *h, int enable, int lc, int minw) {
-    if (!h || lc < 1 || lc > 64 || !(minw == 8 || minw == 12 || minw == 16)) return NECG_ERR_ARG;
-    if (enable && !h->sym_ok) return NECG_ERR_UNSUPPORTED;
-    h->use_sym = enable != 0;
+int necg_set_symmetric(necg_handle *h, int mode, int lc, int minw) {
+    if (!h || mode < 0 || mode > 2 || lc < 1 || lc > 64 || !(minw == 8 || minw == 12 || minw == 16))
+        return NECG_ERR_ARG;
+    if (mode && !h->sym_ok) return NECG_ERR_UNSUPPORTED;
+    h->grad_mode = mode;
     h->lc_s = lc;
     h->minb_s = minw;
     return NECG_OK;
@@ -410,7 +416,26 @@ int necg_outprod(necg_handle *h, int K, const double *x_dev, double *f_dev, doub
     a.H = H_dev ? H_dev : h->d_H;
     a.S = S_dev ? S_dev : h->d_S;
     a.g = g_dev;
-    if (h->use_sym && (rc = ensure_sym_tiles(h, K, st))) return rc;
+    if (h->grad_mode >= 1 && (rc = ensure_sym_tiles(h, K, st))) return rc;
+    if (h->grad_mode == 2) {
+        // fused: one pass over unordered pairs writes H, S and the split gradients
+        a.stiles = h->d_stiles;
+        a.stile_start = h->d_stile_start;
+        a.nstiles = h->nstiles;
+        a.LC_s = h->lc_s;
+        a.psym = h->d_psym;
+        mark(h, 0, st);
+        if (necg::launch_prep(a, st)) return NECG_ERR_UNSUPPORTED;
+        mark(h, 1, st);
+        necg::launch_fsym(a, st);
+        mark(h, 2, st);
+        necg::launch_rows_finalize(a, f_dev, g_dev + siv, 0, 0.0, 0.0, st);
+        mark(h, 3, st);
+        mark(h, 4, st);
+        necg::launch_fsym_reduce(a, st);
+        mark(h, 5, st);
+        return finish_launch();
+    }
     mark(h, 0, st);
     if (necg::launch_prep(a, st)) return NECG_ERR_UNSUPPORTED;
     mark(h, 1, st);

@@ -52,7 +52,18 @@ template <int N> void host_records(std::vector<double> &bra, std::vector<double>
     ket[KL::tMA] = 1.0;
     ket[KL::w] = 1.0;
     ket[KL::wC] = 1.0;
+    ket[KL::winv] = 1.0;
 }
+
+// Ket-side output of one term: put stores, add accumulates (one add counted).
+struct CountRow {
+    double r[64];
+    void put(int f, CD v) { r[f] = v.v; }
+    void add(int f, CD v) {
+        r[f] += v.v;
+        ++count_ctx().flops;
+    }
+};
 
 template <int N> void count_term(int which, long long &flops, long long &special) {
     std::vector<double> bra, ket;
@@ -73,11 +84,29 @@ template <int N> void count_term(int which, long long &flops, long long &special
         CD w(1.0), h(0.0), s(0.0);
         h += w * ov * (2.0 * tau + rho - sig);
         s += w * ov;
-    } else {
+    } else if (which == 1) {
         RegAcc<N, CD> acc;
         acc.zero();
         count_ctx() = CountCtx();  // zeroing the accumulators is not part of a term
         term_grad<N>(b, kr, cs, CD(1.0), CD(0.5), CD(1.0), acc);
+    } else if (which == 2) {
+        RegAcc<N, CD> acc;
+        acc.zero();
+        CountRow ko;
+        count_ctx() = CountCtx();
+        // the ket row's warp column sum and frame map are counted per (l, P),
+        // not per term: they are amortised over the 32 bras of a tile
+        term_sym<N>(b, kr, cs, CD(0.5), CD(1.0), CD(1.0), acc, ko);
+    } else {
+        RegAcc<N, CD> aH, aS;
+        aH.zero();
+        aS.zero();
+        CountRow kH, kS;
+        count_ctx() = CountCtx();
+        CD h, ov, hs(0.0), ss(0.0), w(1.0);
+        term_fused<N>(b, kr, cs, CD(1.0), CD(1.0), aH, aS, kH, kS, h, ov);
+        hs += w * h;  // the pass's sums of w_P h and w_P ov over P
+        ss += w * ov;
     }
     flops = count_ctx().flops;
     special = count_ctx().special;

@@ -26,7 +26,8 @@ struct necg_handle {
     bool profile = false;
     cudaEvent_t ev[6] = {};
     // symmetric gradient pass (when the symmetry set is closed under inverse)
-    bool sym_ok = false, use_sym = false;
+    bool sym_ok = false;
+    int grad_mode = 0;  // 0 ordered pairs, 1 symmetric, 2 fused energy + symmetric
     int lc_s = 4, minb_s = 8;
     int *d_pinv = nullptr;
     int *d_kcnt = nullptr, *d_ksrc = nullptr;

@@ -34,6 +34,10 @@ int launch_energy(const LaunchArgs &a, cudaStream_t st);
 int launch_grad(const LaunchArgs &a, cudaStream_t st);
 int launch_gsym(const LaunchArgs &a, cudaStream_t st);
 int launch_gsym_reduce(const LaunchArgs &a, cudaStream_t st);
+// fused energy + symmetric gradient pass (writes H, S and split partials) and
+// its reduction (needs E in scal, i.e. after launch_rows_finalize)
+int launch_fsym(const LaunchArgs &a, cudaStream_t st);
+int launch_fsym_reduce(const LaunchArgs &a, cudaStream_t st);
 int launch_grad_tiles(const LaunchArgs &a, cudaStream_t st);
 int launch_grad_reduce(const LaunchArgs &a, cudaStream_t st);
 int launch_matel(const LaunchArgs &a, const int *terms, int nterms, double *out, cudaStream_t st);

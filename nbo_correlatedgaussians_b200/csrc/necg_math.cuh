@@ -137,6 +137,7 @@ struct BraRef {
 // Register accumulators of one bra gradient (see term_grad).
 template <int N, typename R> struct RegAcc {
     R G[tri(N)], D, S[3 * N];
+#pragma nv_exec_check_disable
     NECG_HD void zero() {
 #pragma unroll
         for (int t = 0; t < tri(N); ++t) G[t] = R(0.0);
@@ -700,6 +701,156 @@ NECG_HD bool term_sym(const BA &b, const KA &kr, const Consts<N> &cs, R E, R wb,
             }
             acc.g(sx(i, j)) += s;
             kout.add(sx(i, j), -t);
+        }
+    return ok;
+}
+
+// One (k, l, P) term of the fused pass: the H element h and overlap ov (for H
+// and S), and the bra and ket gradients of h and of ov kept apart -- the pass
+// runs before E is known, and g = g_H - E g_S is formed once E is.  With
+// Fb = wb h, ovb = wb ov (Fk, ovk with wk):
+//   bra, H: the formulas of term_grad with Fw = Fb, ovw = ovb
+//   bra, S: d(ov)/dA_k = ov (-Dk Dk^T - 1.5 Bi + 0.75 A_k^-1), d(ov)/ds_k = -2 ov Y
+// and the ket formulas of term_sym with the same split (koH, koS).
+#pragma nv_exec_check_disable
+template <int N, typename R, typename BA, typename KA, typename ACC, typename KOUT>
+NECG_HD bool term_fused(const BA &b, const KA &kr, const Consts<N> &cs, R wb, R wk, ACC &accH, ACC &accS,
+                        KOUT &koH, KOUT &koS, R &h_out, R &ov_out) {
+    using KL = KetLayout<N>;
+    using BL = BraLayout<N>;
+    R Bi[tri(N)], T[3 * N], ov;
+    const bool ok = term_core<N>(b, kr, cs, Bi, T, ov);
+    const R tau = term_tau<N>(b, kr, cs, Bi, T);
+    const R sig = term_sig<N>(cs, T);
+    R Z[3 * N], W[tri(N)], rho;
+    coulomb_grad<N>(Bi, T, cs, rho, Z, W);
+    const R h = ov * (2.0 * tau + rho - sig);
+    h_out = h;
+    ov_out = ov;
+    const R Fb = wb * h, ovb = wb * ov;
+    const R Fk = wk * h, ovk = wk * ov;
+    accH.d() += 0.75 * Fb;
+    accS.d() += 0.75 * ovb;
+    koH.put(tri(N), 0.75 * Fk);
+    koS.put(tri(N), 0.75 * ovk);
+    {
+        R Mt[tri(N)];
+        const R fb = 1.5 * Fb, fk = 1.5 * Fk, sb = 1.5 * ovb, sk = 1.5 * ovk;
+#pragma unroll
+        for (int t = 0; t < tri(N); ++t)
+            Mt[t] = ovb * (6.0 * kr[KL::Np + t] + W[t]) - fb * (b(BL::A + t) + kr[KL::Ap + t]);
+        sandwich<N>(Bi, Mt, [&](int t, R v) { accH.g(t) += v; });
+#pragma unroll
+        for (int t = 0; t < tri(N); ++t)
+            W[t] = ovk * (6.0 * b(BL::Nk + t) + W[t]) - fk * (b(BL::A + t) + kr[KL::Ap + t]);
+        sandwich<N>(Bi, W, [&](int t, R v) { koH.put(t, v); });
+        // S parts: Bi (-1.5 ov B) Bi = -1.5 ov Bi
+#pragma unroll
+        for (int t = 0; t < tri(N); ++t) {
+            accS.g(t) += -(sb * Bi[t]);
+            koS.put(t, -(sk * Bi[t]));
+        }
+    }
+    R Dl[3 * N], Y[3 * N];
+#pragma unroll
+    for (int t = 0; t < 3 * N; ++t) Dl[t] = T[t] - kr[KL::Sp + t];
+    symv3<N>(kr, KL::Ap, Dl, Y);
+    R Zl[3 * N];
+    {
+        R MY[3 * N];
+#pragma unroll
+        for (int i = 0; i < N; ++i)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                R s = cs.M[i * N] * Y[c];
+#pragma unroll
+                for (int k = 1; k < N; ++k) s += cs.M[i * N + k] * Y[3 * k + c];
+                MY[3 * i + c] = s;
+            }
+#pragma unroll
+        for (int i = 0; i < N; ++i)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                R s = b(BL::A + sx(i, 0)) * MY[c];
+#pragma unroll
+                for (int k = 1; k < N; ++k) s += b(BL::A + sx(i, k)) * MY[3 * k + c];
+                Zl[3 * i + c] = Z[3 * i + c] + 4.0 * s;
+            }
+#pragma unroll
+        for (int i = 0; i < N; ++i)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                R s = kr[KL::AMp + i * N] * Y[c];
+#pragma unroll
+                for (int k = 1; k < N; ++k) s += kr[KL::AMp + i * N + k] * Y[3 * k + c];
+                Z[3 * i + c] -= 4.0 * s;
+            }
+    }
+    R Qk[3 * N], Ql[3 * N];
+#pragma unroll
+    for (int i = 0; i < N; ++i)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            R s = Bi[sx(i, 0)] * Z[c], t = Bi[sx(i, 0)] * Zl[c];
+#pragma unroll
+            for (int k = 1; k < N; ++k) {
+                s += Bi[sx(i, k)] * Z[3 * k + c];
+                t += Bi[sx(i, k)] * Zl[3 * k + c];
+            }
+            Qk[3 * i + c] = s;
+            Ql[3 * i + c] = t;
+        }
+    // H: bra s += 2 ovb A_k Qk - 2 Fb Y, ket 2 ovk A_l' Ql + 2 Fk Y ; S: -2 ovb Y, +2 ovk Y
+    {
+        const R ob2 = 2.0 * ovb, fb2 = 2.0 * Fb, ok2 = 2.0 * ovk, fk2 = 2.0 * Fk;
+#pragma unroll
+        for (int i = 0; i < N; ++i)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                R s = b(BL::A + sx(i, 0)) * Qk[c];
+                R t = kr[KL::Ap + sx(i, 0)] * Ql[c];
+#pragma unroll
+                for (int k = 1; k < N; ++k) {
+                    s += b(BL::A + sx(i, k)) * Qk[3 * k + c];
+                    t += kr[KL::Ap + sx(i, k)] * Ql[3 * k + c];
+                }
+                const R y = Y[3 * i + c];
+                accH.s(3 * i + c) += ob2 * s - fb2 * y;
+                accS.s(3 * i + c) += -(ob2 * y);
+                koH.put(tri(N) + 1 + 3 * i + c, ok2 * t + fk2 * y);
+                koS.put(tri(N) + 1 + 3 * i + c, ok2 * y);
+            }
+    }
+    // H: Rk = ovb Qk - Fb/2 Dk, acc += Rk Dk^T + Dk Rk^T ; Rl = ovk Ql + Fk/2 Dl, ket -= Rl Dl^T + Dl Rl^T
+    // S: bra -= ovb Dk Dk^T, ket -= ovk Dl Dl^T
+    {
+        const R fbh = 0.5 * Fb, fkh = 0.5 * Fk;
+#pragma unroll
+        for (int t = 0; t < 3 * N; ++t) {
+            const R dk = b(BL::S + t) - T[t];
+            T[t] = dk;
+            Qk[t] = ovb * Qk[t] - fbh * dk;
+            Ql[t] = ovk * Ql[t] + fkh * Dl[t];
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < N; ++i)
+#pragma unroll
+        for (int j = 0; j <= i; ++j) {
+            R s = Qk[3 * i] * T[3 * j] + T[3 * i] * Qk[3 * j];
+            R t = Ql[3 * i] * Dl[3 * j] + Dl[3 * i] * Ql[3 * j];
+            R dd = T[3 * i] * T[3 * j], ee = Dl[3 * i] * Dl[3 * j];
+#pragma unroll
+            for (int c = 1; c < 3; ++c) {
+                s += Qk[3 * i + c] * T[3 * j + c] + T[3 * i + c] * Qk[3 * j + c];
+                t += Ql[3 * i + c] * Dl[3 * j + c] + Dl[3 * i + c] * Ql[3 * j + c];
+                dd += T[3 * i + c] * T[3 * j + c];
+                ee += Dl[3 * i + c] * Dl[3 * j + c];
+            }
+            accH.g(sx(i, j)) += s;
+            accS.g(sx(i, j)) += -(ovb * dd);
+            koH.add(sx(i, j), -t);
+            koS.add(sx(i, j), -(ovk * ee));
         }
     return ok;
 }

@@ -218,10 +218,11 @@ def boys_f0(z) -> tuple[np.ndarray, np.ndarray]:
 
 
 def term_flops(n: int) -> dict:
-    """Algorithmic FLOPs per (k, l, P) term of the two tile kernels."""
+    """Algorithmic FLOPs per (k, l, P) term: energy, ordered gradient, and one
+    unordered term of the symmetric ("sym") and fused ("fused") passes."""
     L = _lib.lib()
     out = {}
-    for which, name in ((0, "energy"), (1, "grad")):
+    for which, name in ((0, "energy"), (1, "grad"), (2, "sym"), (3, "fused")):
         s = ctypes.c_longlong(0)
         tot = L.necg_term_flops(int(n), which, ctypes.byref(s))
         out[name] = int(tot)

@@ -43,9 +43,10 @@ def workspace_estimate(p: Problem, K_max: int | None = None) -> int:
     bra = tri + 6 * n + tri + 3 + tri
     ps = tri + 1 + 3 * n
     blk = tri + 3 * n
-    # symmetric-pass partials at its narrowest ket chunk (2)
+    # symmetric-pass partials at the tuner's narrowest ket chunk (2), doubled
+    # for the fused pass (H and S partials kept apart)
     ntiles = sum(min(kb * 32 + 31, K - 1) // 2 + 1 for kb in range((K + 31) // 32))
-    sym = ntiles * ps * (32 + 2) if n <= 5 else 0
+    sym = 2 * ntiles * ps * (32 + 2) if n <= 5 else 0
     doubles = (bra * K + ket * K * nst + ps * K * ((K + 3) // 4) + 2 * K * K + 2 * K + 4
                + 2 * (K * blk + K) + 2 + nst * (n * n + 9 * n * n + 1) + sym)
     return 8 * doubles + 3 * 8 * (K * blk + K) + 4096

@@ -77,6 +77,23 @@ def outprod_sym(p, lc_e=4, lc_s=4):
     return rc, float(f[0]), g, H, S
 
 
+def outprod_fused(p, lc_s=4):
+    """The fused energy + symmetric gradient pass emulated on the host."""
+    L = lib()
+    c = _consts(p)
+    x = np.ascontiguousarray(p.x)
+    f = np.zeros(1)
+    g = np.zeros(x.size)
+    H = np.zeros((p.K, p.K))
+    S = np.zeros((p.K, p.K))
+    fn = L.emu_outprod_fused
+    fn.restype = ctypes.c_int
+    rc = fn(ctypes.c_int(p.n), ctypes.c_int(p.nst), ctypes.c_int(p.K), ctypes.c_double(p.efs),
+            *[ctypes.c_void_p(_p(a)) for a in c], ctypes.c_void_p(_p(x)), ctypes.c_int(lc_s),
+            ctypes.c_void_p(_p(f)), ctypes.c_void_p(_p(g)), ctypes.c_void_p(_p(H)), ctypes.c_void_p(_p(S)))
+    return rc, float(f[0]), g, H, S
+
+
 def elements(p, terms):
     L = lib()
     c = _consts(p)

@@ -65,4 +65,11 @@ def test_term_flops_counter(L):
         assert s.value == 3 * n * (n + 1) // 2 + n + 1  # 3 per Coulomb pair, n rsqrt, 1 exp
         prev = g
     assert L.necg_term_flops(5, 1, None) == 3367
+    for n in range(1, 7):
+        e, g, y, f = (L.necg_term_flops(n, w, None) for w in range(4))
+        # an unordered term carries both gradients, so it costs less than two
+        # ordered terms; the fused term adds the H and S elements and the split
+        # S gradient, less than a separate energy term
+        assert g < y < 2 * g
+        assert y < f < y + e
     assert L.necg_term_flops(9, 1, None) == -1

@@ -86,3 +86,26 @@ def test_symmetric_pass_oldquit():
     p = problem_from(d)
     rc, f, g, H, S = emu.outprod_sym(p, 4, 4)
     assert rc == 0 and abs(f - 4.296758204100342) < TOL_E and normwise(g, d["g"]) < TOL_G
+
+
+@pytest.mark.parametrize("system,K,lc_s", [("He", 45, 1), ("He", 45, 6), ("H2", 37, 3), ("H2", 70, 8),
+                                           ("LiH", 33, 4), ("LiH", 40, 7)])
+def test_fused_pass_vs_oracle(system, K, lc_s):
+    """One pass over unordered pairs for H, S and the split H and S gradients,
+    combined as g_H - E g_S once E is known."""
+    p = synth.make_problem(system, K, 11 * K)
+    p.C = np.random.default_rng(K + 1).normal(size=K)
+    fo, go, Ho, So = Oracle.from_problem(p).outprod(p.x, nthreads=8, return_hs=True)
+    rc, f, g, H, S = emu.outprod_fused(p, lc_s)
+    assert rc == 0
+    assert abs(f - fo) < TOL_E
+    assert normwise(g, go) < TOL_G
+    assert np.max(np.abs(H - Ho)) <= TOL_ELEM * max(1.0, np.max(np.abs(Ho)))
+    assert np.max(np.abs(S - So)) <= TOL_ELEM * max(1.0, np.max(np.abs(So)))
+
+
+def test_fused_pass_oldquit():
+    d = golden("oldquit.npz")
+    p = problem_from(d)
+    rc, f, g, H, S = emu.outprod_fused(p, 4)
+    assert rc == 0 and abs(f - 4.296758204100342) < TOL_E and normwise(g, d["g"]) < TOL_G

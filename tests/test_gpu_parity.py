@@ -218,6 +218,55 @@ def test_symmetric_and_ordered_gradient_passes_agree(torch_cuda, system, K):
     assert normwise(gs, go) < 1e-12
 
 
+@pytest.mark.parametrize("system,K,lc", [("He", 80, 3), ("H2", 90, 2), ("LiH", 70, 4), ("LiH", 101, 16)])
+def test_fused_pass_matches_oracle(torch_cuda, system, K, lc):
+    """Mode 2: one pass over unordered pairs writes H and S and the H and S
+    gradients; E, g, H and S against the oracle for each register variant, and
+    the gradient against the two-pass symmetric mode."""
+    import torch
+    from nbo_correlatedgaussians_b200 import _lib, synth
+    p = synth.make_problem(system, K, 7 * K)
+    p.C = np.random.default_rng(K).normal(size=K)
+    eng = _engine(p)
+    L = eng.L
+    assert L.necg_set_symmetric(eng.h, 1, lc, 8) == _lib.NECG_OK
+    f1, g1 = eng.outprod(p.x)
+    fr, gr, Hr, Sr = Oracle.from_problem(p).outprod(p.x, nthreads=8, return_hs=True)
+    for minw in (8, 12, 16):
+        assert L.necg_set_symmetric(eng.h, 2, lc, minw) == _lib.NECG_OK
+        H = torch.empty((K, K), dtype=torch.float64, device=eng.device)
+        S = torch.empty_like(H)
+        fd, gd = eng.outprod_device(torch.from_numpy(p.x), K, H=H, S=S)
+        torch.cuda.synchronize()
+        eng.raise_status("outprod")
+        f2, g2 = eng.outprod(p.x)
+        assert float(fd.item()) == f2 and np.array_equal(gd.cpu().numpy(), g2)
+        assert abs(f2 - fr) < TOL_E and normwise(g2, gr) < TOL_G
+        assert abs(f2 - f1) < TOL_E and normwise(g2, g1) < 1e-12
+        Hn, Sn = H.cpu().numpy(), S.cpu().numpy()
+        assert np.array_equal(Hn, Hn.T) and np.array_equal(Sn, Sn.T)
+        assert np.max(np.abs(Hn - Hr)) <= TOL_ELEM * max(1.0, np.max(np.abs(Hr)))
+        assert np.max(np.abs(Sn - Sr)) <= TOL_ELEM * max(1.0, np.max(np.abs(Sr)))
+
+
+def test_fused_pass_oldquit_and_errors(torch_cuda):
+    """The fused mode on the reference's input file, and the pair-status path
+    (a singular A_k + A_l') leaving the handle usable."""
+    from nbo_correlatedgaussians_b200 import _lib
+    d = golden("oldquit.npz")
+    p = problem_from(d)
+    eng = _engine(p)
+    assert eng.L.necg_set_symmetric(eng.h, 2, 4, 8) == _lib.NECG_OK
+    f, g = eng.outprod(p.x)
+    assert abs(f - 4.296758204100342) < TOL_E and normwise(g, d["g"]) < TOL_G
+    bad = p.copy()
+    bad.iv[2 * p.blk:2 * p.blk + p.svh] = 0.0
+    with pytest.raises(np.linalg.LinAlgError):
+        eng.outprod(bad.x)
+    f2, g2 = eng.outprod(p.x)
+    assert f2 == f and np.array_equal(g2, g)
+
+
 def test_symmetric_pass_unavailable_without_inverse_closure(torch_cuda):
     from nbo_correlatedgaussians_b200 import _lib, synth
     p = synth.make_problem("H2", 20, 4)
