@@ -54,7 +54,15 @@ def parse():
     ap.add_argument("--workload", default="lih_k1024", choices=sorted(WORKLOADS))
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU-baseline sample budget")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--pair-pass", default="auto", choices=["auto", "ordered", "symmetric", "fused"],
+                    help="force the pair pass (auto: the autotuner's choice)")
+    ap.add_argument("--no-tune", action="store_true",
+                    help="skip the autotuner and use the default tiles (for short profiling runs)")
     return ap.parse_args()
+
+
+DEFAULT_TILES = {"lc_e": 2, "minb_e": 16, "lc_g": 4, "minb_g": 8, "sym": 1, "lc_s": 2, "minw_s": 8}
+PASS_MODE = {"ordered": 0, "symmetric": 1, "fused": 2}
 
 
 # ----------------------------------------------------------------------------- CPU port
@@ -210,8 +218,14 @@ def run_engine(args):
     eng = Engine(prob)
     stream = torch.cuda.current_stream()
     x = torch.from_numpy(prob.x).cuda()
-    from nbo_correlatedgaussians_b200.autotune import tuned
-    tiles = tuned(eng, x, prob.K)  # untimed; cached per (GPU, n, nst, K bucket)
+    from nbo_correlatedgaussians_b200.autotune import apply, tuned
+    if args.no_tune:
+        tiles = dict(DEFAULT_TILES)
+    else:
+        tiles = dict(tuned(eng, x, prob.K))  # untimed; cached per (GPU, n, nst, K bucket)
+    if args.pair_pass != "auto":
+        tiles["sym"] = PASS_MODE[args.pair_pass]
+    apply(eng, tiles)
     _lib.check(L.necg_profile(eng.h, 1), "necg_profile")
     g = torch.empty_like(x)
     f = torch.empty(1, dtype=torch.float64, device="cuda")

@@ -124,6 +124,23 @@ int necg_make_grad_dev(necg_handle *h, int K, const double *iv_dev, const double
 int necg_matel(necg_handle *h, int K, const double *iv_dev, int nterms, const int *terms_dev,
                double *out_dev, void *stream);
 
+/* python/rrms.py:21-120 rrms(stfe, stf, ii, jj, n1) for a batch of terms.
+ * terms_dev: nterms * 5 ints (stfe, stf, ii, jj, n1), 1-based (n1 indexes the
+ * 3n Cartesian components, particle-major).  out_dev: nterms * 2 doubles
+ * (ov, st[n1] ov), the symmetry maps applied to both bra and ket. */
+int necg_rrms(necg_handle *h, int K, const double *iv_dev, int nterms, const int *terms_dev,
+              double *out_dev, void *stream);
+
+/* The dipole loop of python/necg.py:200-244: for each Cartesian component m
+ * (particle-major, 3n of them) comps_dev[m] = C^T Hd_m C / C^T Sd C with
+ * Hd_m[j][i] = sum over (stfe, stf) of scvv[stf] scvv[stfe] rrms(stfe, stf, j,
+ * i, m).tk and Sd the same sum of rrms.ov, taken over the lower triangle and
+ * contracted with C on the fly (no K x K matrices).  dipole_dev (3 doubles,
+ * may be NULL) receives sum_i ncv[i] comps[3 (i - 1) + c], the reference's
+ * d7, d8, d9. */
+int necg_dipole(necg_handle *h, int K, const double *iv_dev, const double *C_dev, double *comps_dev,
+                double *dipole_dev, void *stream);
+
 /* python/gradel.py:27-392 gradel(stf, ii, jj) for a batch of terms.
  * tgvl_dev, tgvls_dev: nterms * blk doubles (dH and dS with respect to the bra
  * block [vech(L_ii), s_ii]), doubled when ii == jj as the reference does. */

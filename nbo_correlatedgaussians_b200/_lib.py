@@ -40,6 +40,8 @@ SIGNATURES = [
     ("necg_make_grad_dev", _i, [_vp, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     ("necg_matel", _i, [_vp, _i, _vp, _i, _vp, _vp, _vp]),
     ("necg_gradel", _i, [_vp, _i, _vp, _i, _vp, _vp, _vp, _vp]),
+    ("necg_rrms", _i, [_vp, _i, _vp, _i, _vp, _vp, _vp]),
+    ("necg_dipole", _i, [_vp, _i, _vp, _vp, _vp, _vp, _vp]),
     ("necg_f0", _i, [_vp, _i, _vp, _vp, _vp]),
     ("necg_outprod_noalloc", _i, [_i, _i, _i, _d, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     ("necg_status", _i, [_vp, ctypes.POINTER(_ll)]),

@@ -521,6 +521,41 @@ int necg_matel(necg_handle *h, int K, const double *iv_dev, int nterms, const in
     return finish_launch();
 }
 
+int necg_rrms(necg_handle *h, int K, const double *iv_dev, int nterms, const int *terms_dev,
+              double *out_dev, void *stream) {
+    int rc = check_K(h, K);
+    if (rc) return rc;
+    if (!iv_dev || nterms < 0 || (nterms > 0 && (!terms_dev || !out_dev))) return NECG_ERR_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    if ((rc = begin(h, st))) return rc;
+    LaunchArgs a = base_args(h, K);
+    a.iv = iv_dev;
+    a.C = nullptr;
+    if (necg::launch_prep(a, st)) return NECG_ERR_UNSUPPORTED;
+    if (nterms > 0) necg::launch_rrms(a, terms_dev, nterms, out_dev, st);
+    return finish_launch();
+}
+
+int necg_dipole(necg_handle *h, int K, const double *iv_dev, const double *C_dev, double *comps_dev,
+                double *dipole_dev, void *stream) {
+    int rc = check_K(h, K);
+    if (rc) return rc;
+    if (!iv_dev || !C_dev || !comps_dev) return NECG_ERR_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    if ((rc = begin(h, st))) return rc;
+    if ((rc = ensure_tiles(h, K, st))) return rc;
+    LaunchArgs a = base_args(h, K);
+    // the tile partials reuse the gradient-partial workspace
+    const size_t need = (size_t)a.ntiles * (3 * h->n + 1);
+    const size_t cap = (size_t)necg::part_stride(h->n) * h->K_max * ((h->K_max + 3) / 4);
+    if (need > cap) return NECG_ERR_CAPACITY;
+    a.iv = iv_dev;
+    a.C = C_dev;
+    if (necg::launch_prep(a, st)) return NECG_ERR_UNSUPPORTED;
+    necg::launch_dipole(a, h->d_part, comps_dev, dipole_dev, st);
+    return finish_launch();
+}
+
 int necg_gradel(necg_handle *h, int K, const double *iv_dev, int nterms, const int *terms_dev,
                 double *tgvl_dev, double *tgvls_dev, void *stream) {
     int rc = check_K(h, K);

@@ -298,6 +298,12 @@ __global__ void __launch_bounds__(32, MINW) gsym_kernel(const int2 *__restrict__
 // g_H - E g_S.  Bra partials: part_b[((t * 2 + which) * PS + f) * 32 + lane];
 // ket partials: part_k[((t * LC + l - l0) * 2 + which) * PS + f], which = 0 for
 // H and 1 for S.
+//
+// Shared memory per warp must stay under 228 KB / 8 for 8 resident warps: the
+// ket rows of two lanes are added with one shuffle before they are written,
+// so each of the two ket tables has 16 rows.  The shuffles need the whole warp,
+// so every lane evaluates a term: a lane without a pair (l > k, or k >= K)
+// evaluates the finite pair (l, l, P) with zero weights, which adds nothing.
 template <int N, int MINW>
 __global__ void __launch_bounds__(32, MINW) fsym_kernel(const int2 *__restrict__ tiles, int ntiles,
                                                    int LC, int K, int nst, Consts<N> cs,
@@ -311,7 +317,7 @@ __global__ void __launch_bounds__(32, MINW) fsym_kernel(const int2 *__restrict__
     constexpr int PS = Part<N>::size;
     static_assert(PS <= 32, "the symmetric pass needs tri(n) + 1 + 3n <= 32");
     __shared__ double sacc[2 * PS * 32];
-    __shared__ double krow[2][32 * 33];
+    __shared__ double krow[2][16 * 33];
     __shared__ double kred[32];
     const int t = blockIdx.x;
     const int lane = threadIdx.x;
@@ -325,37 +331,44 @@ __global__ void __launch_bounds__(32, MINW) fsym_kernel(const int2 *__restrict__
     SmemAcc<N> accH{sacc + lane}, accS{sacc + PS * 32 + lane};
     accH.zero();
     accS.zero();
-    const BraRef b{bra + (kval ? k : 0), (size_t)K};
-    struct RowOut {
+    // ket row output: lanes 2i and 2i+1 add their values; lane 2i writes row i
+    struct PairOut {
         double *r;
-        __device__ __forceinline__ void put(int f, double v) { r[f] = v; }
-        __device__ __forceinline__ void add(int f, double v) { r[f] += v; }
-    } koH{krow[0] + lane * 33}, koS{krow[1] + lane * 33};
+        bool lead;
+        __device__ __forceinline__ void put(int f, double v) {
+            v += __shfl_xor_sync(0xffffffffu, v, 1);
+            if (lead) r[f] = v;
+        }
+        __device__ __forceinline__ void add(int f, double v) {
+            v += __shfl_xor_sync(0xffffffffu, v, 1);
+            if (lead) r[f] += v;
+        }
+    } koH{krow[0] + (lane >> 1) * 33, !(lane & 1)}, koS{krow[1] + (lane >> 1) * 33, !(lane & 1)};
     bool ok = true;
     int flags = 0, bad = 0;
     for (int l = l0; l < l1; ++l) {
         double aH = 0.0, aS = 0.0, hsum = 0.0, ssum = 0.0;
         const bool active = kval && l <= k;
+        const BraRef b{bra + (active ? k : l), (size_t)K};
         for (int P = 0; P < nst; ++P) {
             const double *kr = ket + ((size_t)l * nst + P) * KL::size;
+            const double wb = active ? kr[KL::wC] : 0.0;
+            const double wk = active && l < k ? 2.0 * Ck * kr[KL::winv] : 0.0;
+            double h, ov;
+            const bool tok = term_fused<N, double>(b, kr, cs, wb, wk, accH, accS, koH, koS, h, ov);
             if (active) {
-                const double wk = l < k ? 2.0 * Ck * kr[KL::winv] : 0.0;
-                double h, ov;
-                ok = term_fused<N, double>(b, kr, cs, kr[KL::wC], wk, accH, accS, koH, koS, h, ov) && ok;
+                ok = tok && ok;
                 const double w = kr[KL::w];
                 hsum += w * h;
                 ssum += w * ov;
-            } else {
-#pragma unroll
-                for (int f = 0; f < PS; ++f) koH.r[f] = koS.r[f] = 0.0;
             }
             __syncwarp();
 #pragma unroll
             for (int which = 0; which < 2; ++which) {
                 double v = 0.0;
                 if (lane < PS)
-#pragma unroll 8
-                    for (int r = 0; r < 32; ++r) v += krow[which][r * 33 + lane];
+#pragma unroll
+                    for (int r = 0; r < 16; ++r) v += krow[which][r * 33 + lane];
                 kred[lane] = v;
                 __syncwarp();
                 if (lane < PS) {
@@ -470,6 +483,122 @@ __global__ void __launch_bounds__(128) grad_reduce_kernel(const double *__restri
     if (k >= K) return;
     const double sc = scal[1] * (C ? C[k] : 1.0);
     if (!grad_reduce_one<N>(part, 1, K, bra, sc, g, k)) atomicOr(status, 2);
+}
+
+// python/rrms.py:21-120 rrms(stfe, stf, ii, jj, n1) per term: terms[5 t ..] =
+// (stfe, stf, ii, jj, n1), 1-based; out[2 t] = ov, out[2 t + 1] = st[n1] ov.
+template <int N>
+__global__ void __launch_bounds__(128) rrms_kernel(const int *__restrict__ terms, int nterms, int K,
+                                                   int nst, Consts<N> cs,
+                                                   const double *__restrict__ ket,
+                                                   double *__restrict__ out, int *status) {
+    using KL = KetLayout<N>;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nterms) return;
+    const int *q = terms + 5 * t;
+    const int stfe = q[0] - 1, stf = q[1] - 1, ii = q[2] - 1, jj = q[3] - 1, n1 = q[4] - 1;
+    if (stfe < 0 || stfe >= nst || stf < 0 || stf >= nst || ii < 0 || ii >= K || jj < 0 || jj >= K ||
+        n1 < 0 || n1 >= 3 * N) {
+        atomicOr(status, 4);
+        out[2 * t] = out[2 * t + 1] = NAN;
+        return;
+    }
+    double T[3 * N], ov;
+    const bool ok = term_dipole<N, double>(ket + ((size_t)ii * nst + stfe) * KL::size,
+                                           ket + ((size_t)jj * nst + stf) * KL::size, cs, T, ov);
+    double tn = T[0];
+#pragma unroll
+    for (int m = 1; m < 3 * N; ++m)
+        if (m == n1) tn = T[m];
+    out[2 * t] = ov;
+    out[2 * t + 1] = tn * ov;
+    if (!ok) flag_status(status, 1, ii * K + jj);
+}
+
+// Dipole sums of python/necg.py:200-244 contracted with C on the fly, over the
+// energy tiles (lower triangle): for every pair k >= l and every (Pe, P),
+// weight (2 - delta_kl) C_k C_l scvv[Pe] scvv[P]; den += w ov and
+// num[m] += w st[m] ov.  One warp per tile; the warp's sums go to
+// part[t * (3N + 1) + m] (m = 0: den) in a fixed shuffle order.
+template <int N>
+__global__ void __launch_bounds__(32) dipole_kernel(const int2 *__restrict__ tiles, int ntiles, int LC,
+                                                    int K, int nst, Consts<N> cs,
+                                                    const double *__restrict__ ket,
+                                                    const double *__restrict__ C,
+                                                    double *__restrict__ part, int *status) {
+    using KL = KetLayout<N>;
+    constexpr int NM = 3 * N + 1;
+    const int t = blockIdx.x;
+    const int lane = threadIdx.x;
+    if (t >= ntiles) return;
+    const int2 tl = tiles[t];
+    int k, l0, lend;
+    double acc[NM];
+#pragma unroll
+    for (int m = 0; m < NM; ++m) acc[m] = 0.0;
+    bool ok = true;
+    if (energy_lane_range(tl.x, tl.y, lane, LC, K, k, l0, lend)) {
+        const double Ck = C[k];
+        for (int Pe = 0; Pe < nst; ++Pe) {
+            const double *kb = ket + ((size_t)k * nst + Pe) * KL::size;
+            const double wek = kb[KL::w] * Ck;
+            for (int l = l0; l < lend; ++l) {
+                const double wl = (l == k ? 1.0 : 2.0) * wek * C[l];
+                for (int P = 0; P < nst; ++P) {
+                    const double *kr = ket + ((size_t)l * nst + P) * KL::size;
+                    double T[3 * N], ov;
+                    ok = term_dipole<N, double>(kb, kr, cs, T, ov) && ok;
+                    const double wo = wl * kr[KL::w] * ov;
+                    acc[0] += wo;
+#pragma unroll
+                    for (int m = 0; m < 3 * N; ++m) acc[1 + m] += wo * T[m];
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int m = 0; m < NM; ++m) {
+        double v = acc[m];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0) part[(size_t)t * NM + m] = v;
+    }
+    if (!ok) flag_status(status, 1, k * K + l0);
+}
+
+// Sum the dipole tile partials in a fixed order (one block) and form
+// comps[m] = num[m] / den (0 when den = 0, as python/necg.py:228) and the
+// dipole d_c = sum_i ncv[i + 1] comps[3 i + c].
+template <int N>
+__global__ void __launch_bounds__(256) dipole_sum_kernel(const double *__restrict__ part, int ntiles,
+                                                         Consts<N> cs, double *__restrict__ comps,
+                                                         double *__restrict__ dip) {
+    constexpr int NM = 3 * N + 1;
+    __shared__ double red[NM][256];
+    __shared__ double tot[NM];
+    const int j = threadIdx.x;
+#pragma unroll
+    for (int m = 0; m < NM; ++m) {
+        double s = 0.0;
+        for (int t = j; t < ntiles; t += 256) s += part[(size_t)t * NM + m];
+        red[m][j] = s;
+    }
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if (j < w)
+#pragma unroll
+            for (int m = 0; m < NM; ++m) red[m][j] += red[m][j + w];
+        __syncthreads();
+    }
+    if (j < NM) tot[j] = red[j][0];
+    __syncthreads();
+    if (j < 3 * N) comps[j] = tot[0] != 0.0 ? tot[1 + j] / tot[0] : 0.0;
+    __syncthreads();
+    if (j < 3 && dip) {
+        double d = 0.0;
+        for (int i = 0; i < N; ++i) d += cs.q[i] * (tot[0] != 0.0 ? tot[1 + 3 * i + j] / tot[0] : 0.0);
+        dip[j] = d;
+    }
 }
 
 // Per-term elements for the matel / gradel API: terms[3 t .. 3 t + 2] =
@@ -659,6 +788,17 @@ template <int N> struct Launch {
                                                                       a.status);
         }
     }
+    static void rrms(const LaunchArgs &a, const int *terms, int nterms, double *out, cudaStream_t st) {
+        Consts<N> cs = make_consts<N>(a.mass_h, a.ncv_h, a.efs);
+        rrms_kernel<N><<<(nterms + 127) / 128, 128, 0, st>>>(terms, nterms, a.K, a.nst, cs, a.ket, out,
+                                                             a.status);
+    }
+    static void dipole(const LaunchArgs &a, double *part, double *comps, double *dip, cudaStream_t st) {
+        Consts<N> cs = make_consts<N>(a.mass_h, a.ncv_h, a.efs);
+        dipole_kernel<N><<<a.ntiles, 32, 0, st>>>(a.tiles, a.ntiles, a.LC_e, a.K, a.nst, cs, a.ket, a.C, part,
+                                                  a.status);
+        dipole_sum_kernel<N><<<1, 256, 0, st>>>(part, a.ntiles, cs, comps, dip);
+    }
     static void matel(const LaunchArgs &a, const int *terms, int nterms, double *out,
                       cudaStream_t st) {
         Consts<N> cs = make_consts<N>(a.mass_h, a.ncv_h, a.efs);
@@ -722,6 +862,14 @@ int launch_fsym(const LaunchArgs &a, cudaStream_t st) {
 int launch_fsym_reduce(const LaunchArgs &a, cudaStream_t st) {
     if (a.n > 5) return -1;
     NECG_DISPATCH(a.n, fsym_reduce(a, st));
+    return 0;
+}
+int launch_rrms(const LaunchArgs &a, const int *terms, int nterms, double *out, cudaStream_t st) {
+    NECG_DISPATCH(a.n, rrms(a, terms, nterms, out, st));
+    return 0;
+}
+int launch_dipole(const LaunchArgs &a, double *part, double *comps, double *dip, cudaStream_t st) {
+    NECG_DISPATCH(a.n, dipole(a, part, comps, dip, st));
     return 0;
 }
 int launch_matel(const LaunchArgs &a, const int *terms, int nterms, double *out, cudaStream_t st) {

@@ -41,6 +41,10 @@ int launch_fsym_reduce(const LaunchArgs &a, cudaStream_t st);
 int launch_grad_tiles(const LaunchArgs &a, cudaStream_t st);
 int launch_grad_reduce(const LaunchArgs &a, cudaStream_t st);
 int launch_matel(const LaunchArgs &a, const int *terms, int nterms, double *out, cudaStream_t st);
+// dipole: per-term rrms elements, and the C-contracted sums over the energy
+// tiles (part: ntiles * (3n + 1) doubles) reduced into comps[3n] and dip[3]
+int launch_rrms(const LaunchArgs &a, const int *terms, int nterms, double *out, cudaStream_t st);
+int launch_dipole(const LaunchArgs &a, double *part, double *comps, double *dip, cudaStream_t st);
 int launch_gradel(const LaunchArgs &a, const int *terms, int nterms, double *tg, double *tgs,
                   cudaStream_t st);
 // given: 0 compute E and norm from C, H, S; 1 use (eng, norm); 2 read them

@@ -855,4 +855,41 @@ NECG_HD bool term_fused(const BA &b, const KA &kr, const Consts<N> &cs, R wb, R 
     return ok;
 }
 
+// One term of the dipole element of python/rrms.py:21-120 for the bra record
+// (k, Pe) and the ket record (l, P) (both in KetLayout: symmetry applied to both
+// sides): B = A_k'' + A_l', T = Bi (A_k'' s_k'' + A_l' s_l') (rrms's st), and
+// ov = sqrt(8^n) (|L_k| |L_l| / |B|)^{3/2} exp(<e, T> - i1 - i2).  rrms returns
+// (ov, T[n1] ov).  Returns false if B is not positive definite.
+#pragma nv_exec_check_disable
+template <int N, typename R, typename KA, typename KB>
+NECG_HD bool term_dipole(const KA &kb, const KB &kr, const Consts<N> &cs, R (&T)[3 * N], R &ov) {
+    using KL = KetLayout<N>;
+    R Bi[tri(N)], prinv;
+    bool ok;
+    {
+        R B[tri(N)];
+#pragma unroll
+        for (int t = 0; t < tri(N); ++t) B[t] = kb[KL::Ap + t] + kr[KL::Ap + t];
+        ok = chol_inverse<N>(B, Bi, prinv);
+    }
+    R e[3 * N];
+#pragma unroll
+    for (int t = 0; t < 3 * N; ++t) e[t] = kb[KL::ASp + t] + kr[KL::ASp + t];
+#pragma unroll
+    for (int i = 0; i < N; ++i)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            R s = Bi[sx(i, 0)] * e[c];
+#pragma unroll
+            for (int k = 1; k < N; ++k) s += Bi[sx(i, k)] * e[3 * k + c];
+            T[3 * i + c] = s;
+        }
+    R i3 = e[0] * T[0];
+#pragma unroll
+    for (int t = 1; t < 3 * N; ++t) i3 += e[t] * T[t];
+    const R p3 = prinv * prinv * prinv;
+    ov = cs.sqrt8n * kb[KL::pre] * kr[KL::pre] * p3 * exp(i3 - kb[KL::i2] - kr[KL::i2]);
+    return ok;
+}
+
 }  // namespace necg

@@ -192,6 +192,32 @@ class Engine:
         self.raise_status("matel")
         return out.cpu().numpy()
 
+    def rrms(self, iv, terms, K: int | None = None) -> np.ndarray:
+        """(nterms, 2) array of (ov, tk) of python/rrms.py:21; terms are 1-based
+        (stfe, stf, ii, jj, n1)."""
+        iv = self._tensor(iv)
+        K = K or iv.numel() // self.blk
+        t = torch.as_tensor(np.ascontiguousarray(terms, dtype=np.int32).reshape(-1, 5), device=self.device)
+        out = torch.empty((t.shape[0], 2), dtype=torch.float64, device=self.device)
+        rc = self.L.necg_rrms(self.h, K, iv.data_ptr(), t.shape[0], t.data_ptr(), out.data_ptr(),
+                              _stream_ptr(None))
+        _lib.check(rc, "necg_rrms")
+        self.raise_status("rrms")
+        return out.cpu().numpy()
+
+    def dipole(self, iv, C) -> tuple[np.ndarray, np.ndarray]:
+        """(comps, dipole): the 3n component expectation values and the dipole
+        (d_x, d_y, d_z) of python/necg.py:200-244, in atomic units."""
+        iv, C = self._tensor(iv), self._tensor(C)
+        K = C.numel()
+        comps = torch.empty(3 * self.n, dtype=torch.float64, device=self.device)
+        dip = torch.empty(3, dtype=torch.float64, device=self.device)
+        rc = self.L.necg_dipole(self.h, K, iv.data_ptr(), C.data_ptr(), comps.data_ptr(), dip.data_ptr(),
+                                _stream_ptr(None))
+        _lib.check(rc, "necg_dipole")
+        self.raise_status("dipole")
+        return comps.cpu().numpy(), dip.cpu().numpy()
+
     def gradel(self, iv, terms, K: int | None = None):
         """(tgvl, tgvls), each (nterms, blk); terms are 1-based (stf, ii, jj)."""
         iv = self._tensor(iv)

@@ -336,12 +336,15 @@ template <int N> int outprod_fused(const Args &a, const double *x, int LCs, doub
                         ssum[lane] += w * ov.v;
                     }
                 }
+                // the kernel adds lane pairs (2i, 2i+1) by shuffle, then the 16 rows
                 for (int which = 0; which < 2; ++which) {
                     double red[32];
                     for (int j = 0; j < 32; ++j) {
                         double v = 0.0;
                         if (j < PS)
-                            for (int r = 0; r < 32; ++r) v += which ? rowsS[r][j] : rowsH[r][j];
+                            for (int r = 0; r < 16; ++r)
+                                v += which ? rowsS[2 * r][j] + rowsS[2 * r + 1][j]
+                                           : rowsH[2 * r][j] + rowsH[2 * r + 1][j];
                         red[j] = v;
                     }
                     for (int j = 0; j < PS; ++j) (which ? aS : aH)[j] += ket_map_apply(km, P, j, PS, red);

@@ -15,6 +15,14 @@ Fixtures (npz, all FP64):
   f0.npz          f0 / df0 at z on both sides of the 16.3578 branch point and near 0.
   f0_edge.npz     a He problem whose Coulomb argument z sits within 1e-6 of the
                   branch point, with matel / gradel outputs.
+  rrms_<sys>.npz  for He, H2, LiH (K=6): 400 random (stfe, stf, ii, jj, n1)
+                  terms with the rrms outputs (ov, tk).
+  driver_oldquit.npz  the steps of python/necg.py:main on oldquit.dat: the
+                  initial H, S, Kinetic, Potential, lowest eigenpair and
+                  energetics, the L-BFGS-B result (20 iterations, main's
+                  options), the energetics at the optimum and the dipole
+                  components.
+Select generators by name on the command line (default: all).
 The reference is imported only by this script; the tests read the npz files.
 """
 from __future__ import annotations
@@ -34,6 +42,7 @@ import shared as sh  # noqa: E402  (reference module)
 from gradel import gradel  # noqa: E402
 from matel import matel  # noqa: E402
 from outprod import outprod  # noqa: E402
+from rrms import rrms  # noqa: E402
 from read_input import read_input  # noqa: E402
 from utils import df0, f0  # noqa: E402
 from scipy import linalg  # noqa: E402
@@ -171,12 +180,98 @@ def gen_f0_edge():
     print("f0 edge z", out["z_below"], out["z_above"])
 
 
+def gen_rrms(system: str, K: int = 6, nterms: int = 400, seed: int = 13):
+    p = synth.make_problem(system, K, seed)
+    load_into_reference(p)
+    rng = np.random.default_rng(seed)
+    terms = np.stack([rng.integers(1, p.nst + 1, nterms), rng.integers(1, p.nst + 1, nterms),
+                      rng.integers(1, K + 1, nterms), rng.integers(1, K + 1, nterms),
+                      rng.integers(1, 3 * p.n + 1, nterms)], 1).astype(np.int32)
+    terms[:20, 3] = terms[:20, 2]  # diagonal pairs
+    out = np.array([rrms(*map(int, t)) for t in terms])
+    np.savez(os.path.join(HERE, f"rrms_{system}.npz"), terms=terms, rrms=out, **problem_arrays(p))
+    print("rrms", system, out[:2])
+
+
+def _energetics():
+    cHc, cSc = sh.C @ sh.H @ sh.C, sh.C @ sh.S @ sh.C
+    cKc, cPc = sh.C @ sh.Kinetic @ sh.C, sh.C @ sh.Potential @ sh.C
+    return np.array([cHc / cSc, cKc / cSc, cPc / cSc, -2.0 * cKc / cPc])
+
+
+def gen_driver(maxiter: int = 20):
+    """python/necg.py:main on oldquit.dat, step by step, through the reference's
+    own functions (its _build_matrices, scipy's eigh and L-BFGS-B with main's
+    options, its rrms)."""
+    import necg as ref_necg  # noqa: E402  (reference module)
+    from scipy.optimize import minimize
+    read_input(os.path.join(REF, "oldquit.dat"))
+    ref_necg._build_matrices()
+    H0, S0, K0, P0 = sh.H.copy(), sh.S.copy(), sh.Kinetic.copy(), sh.Potential.copy()
+    ev, evec = linalg.eigh(sh.H, sh.S)
+    sh.C[:] = evec[:, 0]
+    C0 = sh.C.copy()
+    en0 = _energetics()
+    hiv = np.concatenate([sh.iv.copy(), sh.C.copy()])
+    fvals = []
+
+    def fun(x):
+        f, g = outprod(x)
+        fvals.append(f)
+        return f, g
+
+    eps = 2.220446649250313e-16
+    res = minimize(fun, hiv, method="L-BFGS-B", jac=True,
+                   options={"maxiter": maxiter, "maxfun": 150 * (sh.siv + sh.M), "ftol": eps,
+                            "gtol": np.sqrt(eps)})
+    sh.iv[:] = res.x[:sh.siv]
+    sh.C[:] = res.x[sh.siv:]
+    ref_necg._build_matrices()
+    en1 = _energetics()
+    # dipole: the loop of python/necg.py:200-244 over its rrms
+    M, nst = sh.M, sh.nst
+    dip = np.zeros(3)
+    den = None
+    comps = np.zeros(3 * sh.ne)
+    for kk in range(1, 3 * sh.ne + 1):
+        hd = np.zeros((M, M))
+        sd = np.zeros((M, M))
+        for stfe in range(1, nst + 1):
+            for stf in range(1, nst + 1):
+                w = sh.scvv[stf - 1] * sh.scvv[stfe - 1]
+                for i in range(1, M + 1):
+                    for j in range(i, M + 1):
+                        ov_r, tk_r = rrms(stfe, stf, j, i, kk)
+                        hd[j - 1, i - 1] += w * tk_r
+                        sd[j - 1, i - 1] += w * ov_r
+        hd = np.tril(hd) + np.tril(hd, -1).T
+        sd = np.tril(sd) + np.tril(sd, -1).T
+        den = sh.C @ sd @ sh.C
+        comps[kk - 1] = (sh.C @ hd @ sh.C) / den if den != 0.0 else 0.0
+        dip[(kk - 1) % 3] += sh.ncv[(kk - 1) // 3 + 1] * comps[kk - 1]
+    np.savez(os.path.join(HERE, "driver_oldquit.npz"), H0=H0, S0=S0, Kin0=K0, Pot0=P0, eig0=ev[0], C0=C0,
+             en0=en0, x_opt=res.x, f_opt=res.fun, nit=res.nit, nfev=res.nfev, fvals=np.array(fvals),
+             en1=en1, dip_comps=comps, dipole=dip, maxiter=maxiter)
+    print("driver: eig0", ev[0], "en0", en0, "f_opt", res.fun, "nit", res.nit, "en1", en1, "dipole", dip)
+
+
 if __name__ == "__main__":
-    gen_f0()
-    gen_f0_edge()
-    gen_oldquit()
-    for system in ("He", "H2", "LiH"):
-        gen_elements(system)
-    gen_outprod("He", 16, 21)
-    gen_outprod("H2", 12, 22)
-    gen_outprod("LiH", 6, 23)
+    want = set(sys.argv[1:]) or {"f0", "f0_edge", "oldquit", "elements", "outprod", "rrms", "driver"}
+    if "f0" in want:
+        gen_f0()
+    if "f0_edge" in want:
+        gen_f0_edge()
+    if "oldquit" in want:
+        gen_oldquit()
+    if "elements" in want:
+        for system in ("He", "H2", "LiH"):
+            gen_elements(system)
+    if "outprod" in want:
+        gen_outprod("He", 16, 21)
+        gen_outprod("H2", 12, 22)
+        gen_outprod("LiH", 6, 23)
+    if "rrms" in want:
+        for system in ("He", "H2", "LiH"):
+            gen_rrms(system)
+    if "driver" in want:
+        gen_driver()
