@@ -1,0 +1,179 @@
+"""Drop-in driver with the flow of python/necg.py:main (itself the analogue of
+source/necg.f90): read the input, build H, S, Kinetic and Potential, solve the
+generalised eigenproblem for the initial C, minimise E over x = [iv, C] with
+L-BFGS-B on ``outprod``, rebuild at the optimum and compute the dipole.
+
+Everything after ``read_input`` stays on the GPU except the optimiser itself
+(SciPy, as in the reference): the matrix build and the dipole run in the CUDA
+library, and the eigenproblem H v = lambda S v is solved on the device
+(Cholesky of S, then the symmetric eigenproblem of L^-1 H L^-T) instead of
+scipy.linalg.eigh on the host (python/necg.py:129-134).
+
+Usage:  python -m nbo_correlatedgaussians_b200.necg [input_file]
+"""
+from __future__ import annotations
+
+import os
+import sys
+import time
+
+import numpy as np
+import torch
+from scipy.optimize import minimize
+
+from . import _state
+from . import shared as sh
+from .outprod import outprod
+from .read_input import read_input
+from .utils import biout, get_current_time
+
+DEBYE = 2.541765e0  # python/necg.py:235
+
+
+def _build_matrices() -> None:
+    """H, S, Kinetic, Potential from the current iv into ``shared``
+    (python/necg.py:36-58), built by the energy tiles on the device."""
+    eng = _state.engine()
+    H, S, Kin, Pot, _ = eng.build_matrices(sh.iv, K=sh.M, parts=True)
+    sh.H, sh.S = H.cpu().numpy(), S.cpu().numpy()
+    sh.Kinetic, sh.Potential = Kin.cpu().numpy(), Pot.cpu().numpy()
+
+
+def _rayleigh_quotient() -> tuple[float, float, float, float]:
+    """(energy, kinetic, potential, virial) at the current C (python/necg.py:61-71)."""
+    C = sh.C
+    cHc, cSc = float(C @ sh.H @ C), float(C @ sh.S @ C)
+    cKc, cPc = float(C @ sh.Kinetic @ C), float(C @ sh.Potential @ C)
+    return cHc / cSc, cKc / cSc, cPc / cSc, -2.0 * (cKc / cSc) / (cPc / cSc)
+
+
+def _print_energetics(energy: float, kin: float, pot: float, virial: float) -> None:
+    print("*" * 69)
+    print()
+    print(f"Rayleigh Quotient: {energy:25.15f}")
+    print()
+    print(f"Average Kinetic  : {kin:25.15f}")
+    print()
+    print(f"Average Potential: {pot:25.15f}")
+    print()
+    print(f"Virial Coef.     : {virial:25.15f}")
+    print()
+    print("*" * 69)
+
+
+def generalized_eigh(H, S, device=None) -> tuple[np.ndarray, np.ndarray]:
+    """All eigenpairs of H v = lambda S v on the GPU, eigenvalues ascending and
+    eigenvectors S-orthonormal (the output of scipy.linalg.eigh(H, S) /
+    LAPACK DSYGV, up to the sign of each vector).  Raises
+    numpy.linalg.LinAlgError if S is not positive definite."""
+    dev = device or _state.engine().device
+    Ht = torch.as_tensor(np.asarray(H), dtype=torch.float64, device=dev)
+    St = torch.as_tensor(np.asarray(S), dtype=torch.float64, device=dev)
+    Lc, info = torch.linalg.cholesky_ex(St)
+    if int(info.item()) != 0:
+        raise np.linalg.LinAlgError("S is not positive definite")
+    A = torch.linalg.solve_triangular(Lc, Ht, upper=False)            # L^-1 H
+    A = torch.linalg.solve_triangular(Lc, A.T.contiguous(), upper=False)  # L^-1 (L^-1 H)^T
+    A = 0.5 * (A + A.T)
+    w, V = torch.linalg.eigh(A)
+    X = torch.linalg.solve_triangular(Lc.T.contiguous(), V, upper=True)  # L^-T V
+    return w.cpu().numpy(), X.cpu().numpy()
+
+
+def dipole() -> tuple[np.ndarray, np.ndarray]:
+    """(components, dipole) at the current iv, C: the 3n component expectation
+    values and (d_x, d_y, d_z) in atomic units (python/necg.py:200-244)."""
+    return _state.engine().dipole(sh.iv, sh.C)
+
+
+def main(input_file: str = "oldquit.dat", maxiter: int = 20, output: str | None = None) -> dict:
+    """Run the driver; returns the quantities it prints (for tests and callers)."""
+    if output is None:
+        output = "necg.out"
+    from . import utils
+    utils._OUTPUT_FILE = output
+    if os.path.exists(output):
+        os.remove(output)
+    biout("N-particle Non-Born-Oppenheimer Correlated Gaussians")
+    biout("=" * 68)
+    biout(":PROGRAM BEGINS:")
+    td, tt, tz = get_current_time()
+    biout(f"Date: {td} | Time: {tt} / {tz} gmt")
+
+    read_input(input_file)
+    print(f"M, NE, NST = {sh.M}, {sh.ne}, {sh.nst}")
+    print(f"Electric Field = {sh.efs}")
+    print(f"OUTPUT FILENAME = {output}")
+    res: dict = {}
+
+    t0 = time.perf_counter()
+    _build_matrices()
+    res["t_matrices"] = time.perf_counter() - t0
+    print(f"Time for matrix calc. is {res['t_matrices']:.3f} seconds")
+
+    try:
+        w, X = generalized_eigh(sh.H, sh.S)
+        print(f"Eigenvalue = {w[0]:.15f}")
+        sh.C[:] = X[:, 0]
+        res["eig0"] = float(w[0])
+    except np.linalg.LinAlgError as exc:
+        print(f"Warning: generalised eigenvalue problem failed: {exc}")
+        res["eig0"] = None
+    res["C0"] = sh.C.copy()
+    print()
+    print("***** The Input Vectors *****")
+    print(sh.C)
+    print("***** End Input Vectors *****")
+    print()
+    res["en0"] = _rayleigh_quotient()
+    _print_energetics(*res["en0"])
+
+    hiv = np.concatenate([sh.iv.copy(), sh.C.copy()])
+    fvals = []
+
+    def fun(x):
+        f, g = outprod(x)
+        fvals.append(f)
+        return f, g
+
+    eps = 2.220446649250313e-16
+    t0 = time.perf_counter()
+    result = minimize(fun, hiv, method="L-BFGS-B", jac=True,
+                      options={"maxiter": maxiter, "maxfun": 150 * (sh.siv + sh.M), "ftol": eps,
+                               "gtol": np.sqrt(eps)})
+    res["t_optimise"] = time.perf_counter() - t0
+    print(f"Time for energy/gradient calc. is {res['t_optimise']:.3f} seconds")
+    print(f"Energy is {result.fun:.15f} hartree")
+    print(f"Optimiser message: {result.message}")
+    res.update(f_opt=float(result.fun), x_opt=result.x.copy(), nit=int(result.nit), nfev=int(result.nfev),
+               fvals=np.array(fvals))
+
+    sh.iv[:] = result.x[:sh.siv]
+    sh.C[:] = result.x[sh.siv:]
+    print()
+    print("***** The Output Vectors *****")
+    print(sh.C)
+    print()
+    print("***** End Output Vectors *****")
+    print()
+    _build_matrices()
+    res["en1"] = _rayleigh_quotient()
+    _print_energetics(*res["en1"])
+
+    t0 = time.perf_counter()
+    comps, dip = dipole()
+    res["t_dipole"] = time.perf_counter() - t0
+    res["dip_comps"], res["dipole"] = comps, dip
+    print()
+    for name, d in zip("xyz", dip):
+        print(f"Dipole {name}-component = {d:.15f}  ( {d * DEBYE:.6f} Debye )")
+        print()
+    print("*" * 69)
+    biout("PROGRAM TERMINATES")
+    td, tt, tz = get_current_time()
+    biout(f"Date: {td} | Time: {tt} / {tz} gmt")
+    return res
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "oldquit.dat")

@@ -14,6 +14,8 @@
  *   outprod         python/outprod.py:20-76
  *   make_grad       python/make_grad.py:18-90
  *   _build_matrices python/necg.py:36-58
+ *   rrms            python/rrms.py:21-120
+ *   dipole loop     python/necg.py:200-244
  * The only liberty taken is that every Kronecker product kron(X, I3) acting on a
  * 3n-vector is written as X acting on the n x 3 matrix view of that vector
  * (row = particle, column = x/y/z); kron(X, I3) has no other entries, so the
@@ -596,6 +598,108 @@ int oracle_grad_rows(const OracleProblem *P, const double *iv, int row0, int str
     return 0;
 }
 
+/* ---- python/rrms.py:21-120 ------------------------------------------------ */
+/* Overlap and the full position vector st = akli ee of one (stfe, stf, ii, jj)
+ * term: the symmetry maps are applied to the ket (stf) and to the bra (stfe).
+ * rrms returns (ov, st[n1 - 1] ov). */
+static int rrms_pair(const OracleProblem *P, const double *iv, int stfe, int stf, int ii, int jj,
+                     double *ov, double st[3 * NX]) {
+    const int n = P->n, svh = n * (n + 1) / 2, skp = 3 * n, blk = svh + skp;
+    const int se = stfe - 1, s0 = stf - 1, i0 = ii - 1, j0 = jj - 1;
+    Mat lk, ell, ak, al, t, sm, smT, tmp;
+    memset(lk, 0, sizeof(Mat));
+    memset(ell, 0, sizeof(Mat));
+    int kk = i0 * blk, ll = j0 * blk; /* python/rrms.py:52-58 */
+    for (int i = 0; i < n; ++i)
+        for (int j = i; j < n; ++j) {
+            lk[j][i] = iv[kk++];
+            ell[j][i] = iv[ll++];
+        }
+    mtr(n, lk, t); mm(n, lk, t, ak); /* python/rrms.py:60-61 */
+    mtr(n, ell, t); mm(n, ell, t, al);
+    for (int i = 0; i < n; ++i) /* ket: al = sml^T (al sml), python/rrms.py:64-65 */
+        for (int j = 0; j < n; ++j) sm[i][j] = P->sml[(size_t)s0 * n * n + i * n + j];
+    mm(n, al, sm, tmp); mtr(n, sm, smT); mm(n, smT, tmp, al);
+    for (int i = 0; i < n; ++i) /* bra: ak = sml_e^T (ak sml_e), python/rrms.py:68-69 */
+        for (int j = 0; j < n; ++j) sm[i][j] = P->sml[(size_t)se * n * n + i * n + j];
+    mm(n, ak, sm, tmp); mtr(n, sm, smT); mm(n, smT, tmp, ak);
+    double s1[3 * NX], s2[3 * NX], s1t[3 * NX], s2t[3 * NX]; /* python/rrms.py:72-79 */
+    for (int k = 0; k < skp; ++k) {
+        s1[k] = iv[i0 * blk + svh + k];
+        s2[k] = iv[j0 * blk + svh + k];
+    }
+    const double *Se = P->sms + (size_t)se * skp * skp, *Sk = P->sms + (size_t)s0 * skp * skp;
+    for (int r = 0; r < skp; ++r) {
+        double a = 0.0, b = 0.0;
+        for (int c = 0; c < skp; ++c) {
+            a += Sk[r * skp + c] * s2[c];
+            b += Se[r * skp + c] * s1[c];
+        }
+        s2t[r] = a;
+        s1t[r] = b;
+    }
+    Vec3 st1, st2, iv1, iv2, ee, stv;
+    for (int i = 0; i < n; ++i)
+        for (int c = 0; c < 3; ++c) {
+            st1[i][c] = s1t[3 * i + c];
+            st2[i][c] = s2t[3 * i + c];
+        }
+    Mat akl, akli; /* python/rrms.py:82-90 */
+    for (int i = 0; i < n; ++i)
+        for (int j = 0; j < n; ++j) akl[i][j] = ak[i][j] + al[i][j];
+    double det;
+    if (lu_inv_det(n, akl, akli, &det) != 0) return -1;
+    const double dett = fabs(det);
+    double pk = 1.0, pl = 1.0;
+    for (int i = 0; i < n; ++i) { pk *= lk[i][i]; pl *= ell[i][i]; }
+    const double detak = sqrt(fabs(pk * pk)), detal = sqrt(fabs(pl * pl));
+    mv3(n, ak, st1, iv1); /* overlap, python/rrms.py:101-116 */
+    const double i1 = dot3(n, st1, iv1);
+    mv3(n, al, st2, iv2);
+    const double i2 = dot3(n, st2, iv2);
+    for (int i = 0; i < n; ++i)
+        for (int c = 0; c < 3; ++c) ee[i][c] = iv1[i][c] + iv2[i][c];
+    mv3(n, akli, ee, stv);
+    const double i3 = dot3(n, ee, stv);
+    const double r = detak * detal / dett;
+    const double prefac = sqrt(pow(8.0, n)) * sqrt(r * r * r);
+    *ov = exp(-(i1 + i2) + i3) * prefac;
+    for (int i = 0; i < n; ++i)
+        for (int c = 0; c < 3; ++c) st[3 * i + c] = stv[i][c];
+    return 0;
+}
+
+int oracle_rrms(const OracleProblem *P, const double *iv, int stfe, int stf, int ii, int jj, int n1,
+                double out[2]) {
+    double ov, st[3 * NX];
+    if (rrms_pair(P, iv, stfe, stf, ii, jj, &ov, st)) return -1;
+    out[0] = ov;
+    out[1] = st[n1 - 1] * ov; /* python/rrms.py:118-120 */
+    return 0;
+}
+
+/* Lower triangles of the dipole matrices of python/necg.py:205-218 for bra
+ * rows j = row0, row0 + stride, ...: hd[(m * K + j - 1) * K + i - 1] for each
+ * component m (the loop's kk - 1) and sd[(j - 1) * K + i - 1].  The reference
+ * calls rrms once per component with the same (ov, st); here one pair
+ * evaluation serves every component. */
+int oracle_dipole_rows(const OracleProblem *P, const double *iv, int row0, int stride, double *hd,
+                       double *sd) {
+    const int K = P->K, nst = P->nst, m3 = 3 * P->n;
+    for (int j = row0; j <= K; j += stride)
+        for (int i = 1; i <= j; ++i)
+            for (int stfe = 1; stfe <= nst; ++stfe)
+                for (int stf = 1; stf <= nst; ++stf) {
+                    double ov, st[3 * NX];
+                    if (rrms_pair(P, iv, stfe, stf, j, i, &ov, st)) return -1;
+                    const double w = P->scvv[stf - 1] * P->scvv[stfe - 1];
+                    const size_t ji = (size_t)(j - 1) * K + (i - 1);
+                    for (int m = 0; m < m3; ++m) hd[(size_t)m * K * K + ji] += w * st[m] * ov;
+                    sd[ji] += w * ov;
+                }
+    return 0;
+}
+
 typedef struct {
     const OracleProblem *P;
     const double *iv;
@@ -607,6 +711,8 @@ static void *job_run(void *arg) {
     Job *j = (Job *)arg;
     if (j->which == 0)
         j->rc = oracle_build_rows(j->P, j->iv, j->row0, j->stride, j->a, j->b, j->c, j->d);
+    else if (j->which == 2)
+        j->rc = oracle_dipole_rows(j->P, j->iv, j->row0, j->stride, j->a, j->b);
     else
         j->rc = oracle_grad_rows(j->P, j->iv, j->row0, j->stride, j->a, j->b);
     return NULL;
@@ -735,4 +841,43 @@ double oracle_sample_terms(const OracleProblem *P, const double *iv, int nmat,
         acc += tg[0] + tgs[0];
     }
     return acc;
+}
+
+/* ---- python/necg.py:200-244 (dipole) --------------------------------------- */
+/* comps[m] = C^T Hd_m C / C^T Sd C (0 if C^T Sd C = 0) with the matrices
+ * symmetrised from their lower triangles; dip[c] = sum_i ncv[i] comps[3(i-1)+c]. */
+int oracle_dipole(const OracleProblem *P, const double *iv, const double *C, int nthreads,
+                  double *comps, double *dip) {
+    const int K = P->K, n = P->n, m3 = 3 * n;
+    const size_t kk = (size_t)K * K, len = (size_t)m3 * kk;
+    double *hd = (double *)calloc(len, sizeof(double));
+    double *sd = (double *)calloc(len, sizeof(double)); /* run_threads sums len entries */
+    if (!hd || !sd) { free(hd); free(sd); return -2; }
+    int rc = run_threads(P, iv, 2, nthreads, len, hd, sd, NULL, NULL);
+    if (rc) { free(hd); free(sd); return rc; }
+    for (int j = 0; j < K; ++j) /* symmetrise, python/necg.py:221-224 */
+        for (int i = 0; i < j; ++i) {
+            sd[(size_t)i * K + j] = sd[(size_t)j * K + i];
+            for (int m = 0; m < m3; ++m) hd[m * kk + (size_t)i * K + j] = hd[m * kk + (size_t)j * K + i];
+        }
+    double cSc = 0.0;
+    for (int a = 0; a < K; ++a) {
+        double r = 0.0;
+        for (int b = 0; b < K; ++b) r += sd[(size_t)a * K + b] * C[b];
+        cSc += C[a] * r;
+    }
+    for (int c = 0; c < 3; ++c) dip[c] = 0.0;
+    for (int m = 0; m < m3; ++m) {
+        double cHc = 0.0;
+        for (int a = 0; a < K; ++a) {
+            double r = 0.0;
+            for (int b = 0; b < K; ++b) r += hd[m * kk + (size_t)a * K + b] * C[b];
+            cHc += C[a] * r;
+        }
+        comps[m] = cSc != 0.0 ? cHc / cSc : 0.0;
+        dip[m % 3] += P->ncv[m / 3 + 1] * comps[m];
+    }
+    free(hd);
+    free(sd);
+    return 0;
 }

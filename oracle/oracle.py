@@ -6,7 +6,8 @@ never imports it.
 
 The oracle restates the reference Python path (python/matel.py:28-210,
 python/gradel.py:27-392, python/outprod.py:20-76, python/make_grad.py:18-90,
-python/utils.py:78-106) in C; see the header of ``necg_oracle.c``.
+python/utils.py:78-106, python/rrms.py:21-120 and the dipole loop of
+python/necg.py:200-244) in C; see the header of ``necg_oracle.c``.
 """
 from __future__ import annotations
 
@@ -54,6 +55,9 @@ def lib():
         L.oracle_gradel.argtypes = [P, _dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp, _dp]
         L.oracle_build_matrices.argtypes = [P, _dp, ctypes.c_int, _dp, _dp, _dp, _dp]
         L.oracle_outprod.argtypes = [P, _dp, ctypes.c_int, _dp, _dp, _dp, _dp]
+        L.oracle_rrms.argtypes = [P, _dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                  _dp]
+        L.oracle_dipole.argtypes = [P, _dp, _dp, ctypes.c_int, _dp, _dp]
         L.oracle_sample_terms.restype = ctypes.c_double
         L.oracle_sample_terms.argtypes = [P, _dp, ctypes.c_int, _ip, ctypes.c_int, _ip]
         _lib = L
@@ -107,6 +111,26 @@ class Oracle:
         if rc:
             raise np.linalg.LinAlgError("singular matrix in oracle gradel")
         return tg, tgs
+
+    def rrms(self, iv, stfe, stf, ii, jj, n1):
+        iv = np.ascontiguousarray(iv, dtype=np.float64)
+        out = np.zeros(2)
+        rc = lib().oracle_rrms(ctypes.byref(self._p), _ptr(iv), int(stfe), int(stf), int(ii), int(jj), int(n1),
+                               _ptr(out))
+        if rc:
+            raise np.linalg.LinAlgError("singular matrix in oracle rrms")
+        return tuple(out)
+
+    def dipole(self, iv, C, nthreads=1):
+        """(comps (3n,), dipole (3,)) of the dipole loop of python/necg.py:200-244."""
+        iv = np.ascontiguousarray(iv, dtype=np.float64)
+        C = np.ascontiguousarray(C, dtype=np.float64)
+        comps = np.zeros(3 * self.n)
+        dip = np.zeros(3)
+        rc = lib().oracle_dipole(ctypes.byref(self._p), _ptr(iv), _ptr(C), int(nthreads), _ptr(comps), _ptr(dip))
+        if rc:
+            raise np.linalg.LinAlgError("oracle dipole failed")
+        return comps, dip
 
     def build_matrices(self, iv, nthreads=1):
         iv = np.ascontiguousarray(iv, dtype=np.float64)

@@ -41,3 +41,13 @@ def elem_rel(got, ref, ov_ref=None, efs=0.0) -> np.ndarray:
     floor = np.full(ref.shape, 1e-300)
     floor[:, 3] = np.maximum(np.abs(ref[:, 0] * efs), 1e-300)
     return np.abs(got - ref) / np.maximum(np.abs(ref), floor)
+
+
+def rrms_rel(got, ref) -> np.ndarray:
+    """Per-element relative error of (ov, tk) rows of rrms.  tk = st[n1] ov, and a
+    component of the position vector st can cancel to ~0 (rounding-level values
+    of either sign), so the tk floor is 1e-4 |ov| (st components are O(0.1))."""
+    got, ref = np.asarray(got), np.asarray(ref)
+    floor = np.full(ref.shape, 1e-300)
+    floor[:, 1] = np.maximum(1e-4 * np.abs(ref[:, 0]), 1e-300)
+    return np.abs(got - ref) / np.maximum(np.abs(ref), floor)

@@ -94,6 +94,33 @@ def outprod_fused(p, lc_s=4):
     return rc, float(f[0]), g, H, S
 
 
+def rrms(p, terms):
+    L = lib()
+    c = _consts(p)
+    t = np.ascontiguousarray(terms, dtype=np.int32).reshape(-1, 5)
+    out = np.zeros((len(t), 2))
+    fn = L.emu_rrms
+    fn.restype = ctypes.c_int
+    rc = fn(ctypes.c_int(p.n), ctypes.c_int(p.nst), ctypes.c_int(p.K), ctypes.c_double(p.efs),
+            *[ctypes.c_void_p(_p(a)) for a in c], ctypes.c_void_p(_p(np.ascontiguousarray(p.iv))),
+            ctypes.c_int(len(t)), ctypes.c_void_p(_p(t)), ctypes.c_void_p(_p(out)))
+    return rc, out
+
+
+def dipole(p, lc=2):
+    L = lib()
+    c = _consts(p)
+    comps = np.zeros(3 * p.n)
+    dip = np.zeros(3)
+    fn = L.emu_dipole
+    fn.restype = ctypes.c_int
+    rc = fn(ctypes.c_int(p.n), ctypes.c_int(p.nst), ctypes.c_int(p.K), ctypes.c_double(p.efs),
+            *[ctypes.c_void_p(_p(a)) for a in c], ctypes.c_void_p(_p(np.ascontiguousarray(p.iv))),
+            ctypes.c_void_p(_p(np.ascontiguousarray(p.C))), ctypes.c_int(lc), ctypes.c_void_p(_p(comps)),
+            ctypes.c_void_p(_p(dip)))
+    return rc, comps, dip
+
+
 def elements(p, terms):
     L = lib()
     c = _consts(p)

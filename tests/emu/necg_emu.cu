@@ -416,6 +416,92 @@ template <int N> int outprod_fused(const Args &a, const double *x, int LCs, doub
     return flags;
 }
 
+// Host mirror of rrms_kernel (per term) and of dipole_kernel + dipole_sum_kernel
+// (energy tiles in the device list order, per-lane sums over (Pe, l, P), the
+// warp's butterfly sum, tile partials summed by 256 strided threads and a tree).
+template <int N> int rrms_terms(const Args &a, const double *iv, int nterms, const int *terms, double *out) {
+    using KL = KetLayout<N>;
+    Consts<N> cs = consts<N>(a.mass, a.ncv, a.efs);
+    std::vector<double> bra, ket;
+    prep<N>(a, iv, nullptr, bra, ket, cs);
+    int flags = 0;
+    for (int t = 0; t < nterms; ++t) {
+        const int *q = terms + 5 * t;
+        const int stfe = q[0] - 1, stf = q[1] - 1, ii = q[2] - 1, jj = q[3] - 1, n1 = q[4] - 1;
+        CD T[3 * N], ov;
+        if (!term_dipole<N, CD>(HostKet{ket.data() + ((size_t)ii * a.nst + stfe) * KL::size},
+                                HostKet{ket.data() + ((size_t)jj * a.nst + stf) * KL::size}, cs, T, ov))
+            flags |= 1;
+        out[2 * t] = ov.v;
+        out[2 * t + 1] = T[n1].v * ov.v;
+    }
+    return flags;
+}
+
+template <int N> int dipole(const Args &a, const double *iv, const double *C, int LC, double *comps, double *dip) {
+    using KL = KetLayout<N>;
+    constexpr int NM = 3 * N + 1;
+    const int K = a.K, nst = a.nst;
+    Consts<N> cs = consts<N>(a.mass, a.ncv, a.efs);
+    std::vector<double> bra, ket;
+    prep<N>(a, iv, C, bra, ket, cs);
+    int flags = 0;
+    std::vector<double> part;
+    for (int kb = 0; kb * 32 < K; ++kb)
+        for (int lc = 0; lc * LC <= kb * 32 + 31 && lc * LC < K; ++lc) {
+            double acc[32][NM] = {};
+            for (int lane = 0; lane < 32; ++lane) {
+                int k, l0, lend;
+                if (!energy_lane_range(kb, lc, lane, LC, K, k, l0, lend)) continue;
+                for (int Pe = 0; Pe < nst; ++Pe) {
+                    const double *kbr = ket.data() + ((size_t)k * nst + Pe) * KL::size;
+                    const double wek = kbr[KL::w] * C[k];
+                    for (int l = l0; l < lend; ++l) {
+                        const double wl = (l == k ? 1.0 : 2.0) * wek * C[l];
+                        for (int P = 0; P < nst; ++P) {
+                            const double *kr = ket.data() + ((size_t)l * nst + P) * KL::size;
+                            CD T[3 * N], ov;
+                            if (!term_dipole<N, CD>(HostKet{kbr}, HostKet{kr}, cs, T, ov)) flags |= 1;
+                            const double wo = wl * kr[KL::w] * ov.v;
+                            acc[lane][0] += wo;
+                            for (int m = 0; m < 3 * N; ++m) acc[lane][1 + m] += wo * T[m].v;
+                        }
+                    }
+                }
+            }
+            for (int m = 0; m < NM; ++m) {  // butterfly: xor 16, 8, 4, 2, 1
+                double v[32];
+                for (int lane = 0; lane < 32; ++lane) v[lane] = acc[lane][m];
+                for (int o = 16; o > 0; o >>= 1) {
+                    double w[32];
+                    for (int lane = 0; lane < 32; ++lane) w[lane] = v[lane] + v[lane ^ o];
+                    for (int lane = 0; lane < 32; ++lane) v[lane] = w[lane];
+                }
+                part.push_back(v[0]);
+            }
+        }
+    const int ntiles = (int)(part.size() / NM);
+    double tot[NM];
+    for (int m = 0; m < NM; ++m) {
+        double red[256];
+        for (int j = 0; j < 256; ++j) {
+            double s = 0.0;
+            for (int t = j; t < ntiles; t += 256) s += part[(size_t)t * NM + m];
+            red[j] = s;
+        }
+        for (int w = 128; w > 0; w >>= 1)
+            for (int j = 0; j < w; ++j) red[j] += red[j + w];
+        tot[m] = red[0];
+    }
+    for (int m = 0; m < 3 * N; ++m) comps[m] = tot[0] != 0.0 ? tot[1 + m] / tot[0] : 0.0;
+    for (int c = 0; c < 3; ++c) {
+        double d = 0.0;
+        for (int i = 0; i < N; ++i) d += cs.q[i] * comps[3 * i + c];
+        dip[c] = d;
+    }
+    return flags;
+}
+
 template <int N>
 int elements(const Args &a, const double *iv, int nterms, const int *terms, double *mat,
              double *tg, double *tgs) {
@@ -469,6 +555,20 @@ extern "C" int emu_outprod_fused(int n, int nst, int K, double efs, const double
                                  int lc_s, double *f, double *g, double *H, double *S) {
     Args a{nst, K, efs, mass, ncv, scvv, sml, sms};
     EMU_DISPATCH(n, (outprod_fused<N>(a, x, lc_s, f, g, H, S)));
+}
+
+extern "C" int emu_rrms(int n, int nst, int K, double efs, const double *mass, const double *ncv,
+                        const double *scvv, const double *sml, const double *sms, const double *iv, int nterms,
+                        const int *terms, double *out) {
+    Args a{nst, K, efs, mass, ncv, scvv, sml, sms};
+    EMU_DISPATCH(n, (rrms_terms<N>(a, iv, nterms, terms, out)));
+}
+
+extern "C" int emu_dipole(int n, int nst, int K, double efs, const double *mass, const double *ncv,
+                          const double *scvv, const double *sml, const double *sms, const double *iv,
+                          const double *C, int lc, double *comps, double *dip) {
+    Args a{nst, K, efs, mass, ncv, scvv, sml, sms};
+    EMU_DISPATCH(n, (dipole<N>(a, iv, C, lc, comps, dip)));
 }
 
 extern "C" int emu_elements(int n, int nst, int K, double efs, const double *mass, const double *ncv,

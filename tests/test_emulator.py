@@ -8,7 +8,7 @@ import pytest
 from emu import emu
 from oracle.oracle import Oracle
 from nbo_correlatedgaussians_b200 import synth
-from _util import TOL_E, TOL_ELEM, TOL_G, elem_rel, golden, normwise, problem_from
+from _util import TOL_E, TOL_ELEM, TOL_G, elem_rel, golden, normwise, problem_from, rrms_rel
 
 
 @pytest.mark.parametrize("system", ["He", "H2", "LiH"])
@@ -109,3 +109,33 @@ def test_fused_pass_oldquit():
     p = problem_from(d)
     rc, f, g, H, S = emu.outprod_fused(p, 4)
     assert rc == 0 and abs(f - 4.296758204100342) < TOL_E and normwise(g, d["g"]) < TOL_G
+
+
+@pytest.mark.parametrize("system", ["He", "H2", "LiH"])
+def test_rrms_terms_vs_golden(system):
+    d = golden(f"rrms_{system}.npz")
+    rc, out = emu.rrms(problem_from(d), d["terms"])
+    assert rc == 0 and rrms_rel(out, d["rrms"]).max() < TOL_ELEM
+
+
+@pytest.mark.parametrize("system,K,lc", [("He", 45, 2), ("H2", 37, 3), ("LiH", 20, 4)])
+def test_dipole_vs_oracle(system, K, lc):
+    """The dipole tiles (lower triangle, nst^2 symmetry pairs, C contracted on
+    the fly) against the oracle's matrices of python/necg.py:200-244."""
+    p = synth.make_problem(system, K, 17 * K)
+    p.C = np.random.default_rng(K).normal(size=K)
+    comps_o, dip_o = Oracle.from_problem(p).dipole(p.iv, p.C, nthreads=8)
+    rc, comps, dip = emu.dipole(p, lc)
+    assert rc == 0
+    scale = max(np.max(np.abs(comps_o)), 1e-300)
+    assert np.max(np.abs(comps - comps_o)) <= 1e-11 * scale
+    assert np.max(np.abs(dip - dip_o)) <= 1e-11 * max(np.max(np.abs(dip_o)), scale)
+
+
+def test_dipole_oldquit_optimum():
+    d = golden("driver_oldquit.npz")
+    p = problem_from(golden("oldquit.npz"))
+    x = d["x_opt"]
+    p.iv, p.C = x[:p.K * p.blk].copy(), x[p.K * p.blk:].copy()
+    rc, comps, dip = emu.dipole(p, 4)
+    assert rc == 0 and np.max(np.abs(comps - d["dip_comps"])) < 1e-12 and np.max(np.abs(dip - d["dipole"])) < 1e-12

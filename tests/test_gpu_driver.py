@@ -1,0 +1,105 @@
+"""The driver path on the GPU: rrms and the dipole kernel (python/rrms.py:21,
+python/necg.py:200-244) through the C ABI against the reference's goldens and
+the oracle, the device eigensolve, and the whole driver
+(python/necg.py:main) on the reference's input file."""
+import numpy as np
+import pytest
+
+from oracle.oracle import Oracle
+from _util import TOL_E, TOL_ELEM, golden, normwise, problem_from, rrms_rel
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def torch_cuda():
+    import torch
+    assert torch.cuda.is_available()
+    return torch
+
+
+def _engine(p, K_max=None):
+    from nbo_correlatedgaussians_b200.engine import Engine
+    return Engine(p, K_max=K_max or p.K)
+
+
+@pytest.mark.parametrize("system", ["He", "H2", "LiH"])
+def test_rrms_golden(torch_cuda, system):
+    d = golden(f"rrms_{system}.npz")
+    p = problem_from(d)
+    out = _engine(p).rrms(p.iv, d["terms"])
+    assert rrms_rel(out, d["rrms"]).max() < TOL_ELEM
+
+
+def test_rrms_bad_index_raises(torch_cuda):
+    from nbo_correlatedgaussians_b200 import _lib
+    d = golden("rrms_He.npz")
+    p = problem_from(d)
+    eng = _engine(p)
+    with pytest.raises(_lib.NecgError):
+        eng.rrms(p.iv, [[1, 1, 1, 1, 3 * p.n + 1]])  # n1 past the last component
+    out = eng.rrms(p.iv, d["terms"][:4])  # the handle stays usable
+    assert rrms_rel(out, d["rrms"][:4]).max() < TOL_ELEM
+
+
+@pytest.mark.parametrize("system,K,lc", [("He", 80, 2), ("He", 80, 7), ("H2", 64, 4), ("LiH", 40, 2),
+                                         ("LiH", 33, 16)])
+def test_dipole_vs_oracle(torch_cuda, system, K, lc):
+    from nbo_correlatedgaussians_b200 import synth
+    p = synth.make_problem(system, K, 19 * K)
+    p.C = np.random.default_rng(K).normal(size=K)
+    eng = _engine(p)
+    eng.set_tiles(lc, 16)
+    comps, dip = eng.dipole(p.iv, p.C)
+    comps_o, dip_o = Oracle.from_problem(p).dipole(p.iv, p.C, nthreads=8)
+    scale = max(np.max(np.abs(comps_o)), 1e-300)
+    assert np.max(np.abs(comps - comps_o)) <= 1e-11 * scale
+    assert np.max(np.abs(dip - dip_o)) <= 1e-11 * max(np.max(np.abs(dip_o)), scale)
+    c2, d2 = eng.dipole(p.iv, p.C)  # deterministic: fixed reduction order
+    assert np.array_equal(c2, comps) and np.array_equal(d2, dip)
+
+
+def test_dipole_oldquit_optimum(torch_cuda):
+    d = golden("driver_oldquit.npz")
+    p = problem_from(golden("oldquit.npz"))
+    x = d["x_opt"]
+    comps, dip = _engine(p).dipole(x[:p.K * p.blk], x[p.K * p.blk:])
+    assert np.max(np.abs(comps - d["dip_comps"])) < 1e-12
+    assert np.max(np.abs(dip - d["dipole"])) < 1e-12
+
+
+def test_generalized_eigh(torch_cuda):
+    """Device Cholesky + eigh against the reference's scipy.linalg.eigh(H, S)."""
+    from nbo_correlatedgaussians_b200.necg import generalized_eigh
+    d = golden("driver_oldquit.npz")
+    w, X = generalized_eigh(d["H0"], d["S0"], device="cuda")
+    assert abs(w[0] - float(d["eig0"])) < TOL_E
+    c = X[:, 0] * np.sign(X[:, 0] @ d["C0"])  # eigenvectors are defined up to sign
+    assert normwise(c, d["C0"]) < 1e-9
+    assert np.allclose(X.T @ d["S0"] @ X, np.eye(len(w)), atol=1e-10)
+
+
+def test_driver_main_oldquit(torch_cuda, tmp_path):
+    """python/necg.py:main on oldquit.dat: initial eigenpair and energetics, the
+    20 L-BFGS-B iterations (same options), energetics at the optimum, dipole.
+    The optimiser path is reproducible: the oracle-driven run of the same
+    iterations lands within 1e-12 Eh of the reference's."""
+    from nbo_correlatedgaussians_b200 import problem as pr
+    from nbo_correlatedgaussians_b200.necg import main
+    d = golden("driver_oldquit.npz")
+    p = problem_from(golden("oldquit.npz"))
+    path = tmp_path / "oldquit.dat"
+    pr.write_oldquit(p, str(path))
+    res = main(str(path), maxiter=int(d["maxiter"]), output=str(tmp_path / "necg.out"))
+    assert abs(res["eig0"] - float(d["eig0"])) < TOL_E
+    en0, en1 = np.array(res["en0"]), np.array(res["en1"])
+    assert abs(en0[0] - d["en0"][0]) < TOL_E and normwise(en0, d["en0"]) < 1e-9
+    assert res["nit"] == int(d["nit"])
+    assert abs(res["f_opt"] - float(d["f_opt"])) < 1e-9
+    x = res["x_opt"].copy()
+    K = p.K
+    x[p.K * p.blk:] *= np.sign(x[K * p.blk:] @ d["x_opt"][K * p.blk:])
+    assert normwise(x, d["x_opt"]) < 1e-7
+    assert abs(en1[0] - d["en1"][0]) < 1e-9 and normwise(en1, d["en1"]) < 1e-8
+    assert np.max(np.abs(res["dipole"] - d["dipole"])) < 1e-7
+    assert (tmp_path / "necg.out").read_text().strip().endswith("gmt")

@@ -4,7 +4,7 @@ import numpy as np
 import pytest
 
 from oracle.oracle import Oracle
-from _util import TOL_E, TOL_ELEM, elem_rel, golden, normwise, problem_from
+from _util import TOL_E, TOL_ELEM, elem_rel, golden, normwise, problem_from, rrms_rel
 
 
 def test_f0_df0():
@@ -75,3 +75,30 @@ def test_threaded_equals_serial():
     f1, g1 = o.outprod(p.x, nthreads=1)
     f3, g3 = o.outprod(p.x, nthreads=3)
     assert abs(f1 - f3) < 1e-13 and normwise(g3, g1) < 1e-13
+
+
+@pytest.mark.parametrize("system", ["He", "H2", "LiH"])
+def test_rrms(system):
+    """rrms (python/rrms.py:21) on 400 terms, symmetry maps on both sides."""
+    d = golden(f"rrms_{system}.npz")
+    p = problem_from(d)
+    o = Oracle.from_problem(p)
+    out = np.array([o.rrms(p.iv, *t) for t in d["terms"]])
+    assert rrms_rel(out, d["rrms"]).max() < TOL_ELEM
+
+
+def test_driver_steps_oldquit():
+    """The matrices, eigenpair and energetics of python/necg.py:main on
+    oldquit.dat, and the dipole at the reference's L-BFGS-B optimum."""
+    d = golden("driver_oldquit.npz")
+    q = golden("oldquit.npz")
+    p = problem_from(q)
+    o = Oracle.from_problem(p)
+    H, S, Kin, Pot = o.build_matrices(p.iv, nthreads=4)
+    for got, ref in ((H, d["H0"]), (S, d["S0"]), (Kin, d["Kin0"]), (Pot, d["Pot0"])):
+        assert np.max(np.abs(got - ref)) <= TOL_ELEM * np.max(np.abs(ref))
+    K = p.K
+    x = d["x_opt"]
+    comps, dip = o.dipole(x[:K * p.blk], x[K * p.blk:], nthreads=4)
+    assert np.max(np.abs(comps - d["dip_comps"])) < 1e-12
+    assert np.max(np.abs(dip - d["dipole"])) < 1e-12
