@@ -80,7 +80,9 @@ int necg_set_variant(necg_handle *h, int minw_energy, int minw_grad);
  * the gradient-only entry points use mode 1).  Modes 1 and 2 need a symmetry
  * set closed under inverse (each sml and sms has its inverse in the set) and
  * n <= 5; otherwise NECG_ERR_UNSUPPORTED.  lc: kets per tile (1..64); minw: 8,
- * 12 or 16 warps per SM.  Set by the autotuner. */
+ * 12 or 16 warps per SM, and for mode 2 also 108 and 112 (8 and 12 warps with
+ * the ket records re-read at each use instead of held in registers).  Set by
+ * the autotuner. */
 int necg_set_symmetric(necg_handle *h, int mode, int lc, int minw);
 
 /* One objective evaluation: python/outprod.py:20-76 outprod(x) -> (f, g),

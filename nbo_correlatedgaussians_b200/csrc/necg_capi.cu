@@ -361,8 +361,8 @@ int necg_set_tiles(necg_handle *h, int lc_energy, int lc_grad) {
 }
 
 int necg_set_symmetric(necg_handle *h, int mode, int lc, int minw) {
-    if (!h || mode < 0 || mode > 2 || lc < 1 || lc > 64 || !(minw == 8 || minw == 12 || minw == 16))
-        return NECG_ERR_ARG;
+    const bool okw = minw == 8 || minw == 12 || minw == 16 || (mode == 2 && (minw == 108 || minw == 112));
+    if (!h || mode < 0 || mode > 2 || lc < 1 || lc > 64 || !okw) return NECG_ERR_ARG;
     if (mode && !h->sym_ok) return NECG_ERR_UNSUPPORTED;
     h->grad_mode = mode;
     h->lc_s = lc;

@@ -1,0 +1,183 @@
+// necg_device.cuh -- device-side pieces shared by the single-instance kernels
+// (necg_kernels.cu) and the batched persistent kernels (necg_batch.cu): the
+// shared-memory accumulators, the status word, and the body of one tile of the
+// fused pass.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "necg_lanes.cuh"
+#include "necg_math.cuh"
+
+namespace necg {
+
+// Gradient accumulators of one lane in shared memory, interleaved by lane
+// (field t of lane j at t * 32 + j): conflict-free, and not held in registers.
+template <int N> struct SmemAcc {
+    double *p;  // shared base + lane
+    __device__ __forceinline__ void zero() {
+#pragma unroll
+        for (int t = 0; t < Part<N>::size; ++t) p[t * 32] = 0.0;
+    }
+    __device__ __forceinline__ double &g(int t) { return p[t * 32]; }
+    __device__ __forceinline__ double &d() { return p[tri(N) * 32]; }
+    __device__ __forceinline__ double &s(int t) { return p[(tri(N) + 1 + t) * 32]; }
+};
+
+// Status word: [0] bit flags, [1] first failing pair (row-major k*K + l).
+__device__ __forceinline__ void flag_status(int *status, int flags, int pair) {
+    if (!flags) return;
+    atomicOr(status, flags);
+    atomicMin(status + 1, pair);
+}
+
+// Shared memory of one warp's fused tile: bra accumulators for H and S
+// (2 * PS * 32 doubles), two ket tables of 16 rows (2 * 16 * 33) and one
+// reduction row (32).  Sized by the caller for its largest n.
+struct FusedSmem {
+    double *sacc, *krow, *kred;
+};
+
+// One tile of the fused pass over unordered pairs (k >= l): the symmetric
+// gradient pass merged with the energy pass.  Each term gives the H element and
+// overlap (summed over P into H_kl = H_lk and S_kl = S_lk) and the bra and ket
+// gradients of h and of ov kept apart, since E is not known until finalize
+// has run on the H and S this pass writes; the partial sum combines them as
+// g_H - E g_S.  Tile t = (kb, lc): bras k = 32 kb + lane, kets l in
+// [lc LC, lc LC + LC).  Bra partials: part_b[((t * 2 + which) * PS + f) * 32 +
+// lane]; ket partials: part_k[((t * LC + l - l0) * 2 + which) * PS + f], which
+// = 0 for H and 1 for S.
+//
+// Shared memory per warp must stay under 228 KB / 8 for 8 resident warps: the
+// ket rows of two lanes are added with one shuffle before they are written,
+// so each of the two ket tables has 16 rows.  The shuffles need the whole warp,
+// so every lane evaluates a term: a lane without a pair (l > k, or k >= K)
+// evaluates the finite pair (l, l, P) with zero weights, which adds nothing.
+// VKET: ket records re-read at each use (fewer live registers).
+template <int N, bool VKET>
+__device__ __forceinline__ void fsym_tile(int t, int2 tl, int LC, int K, int nst, const Consts<N> &cs,
+                                          const double *__restrict__ bra, const double *__restrict__ ket,
+                                          const double *__restrict__ C, const KetMap &kmap,
+                                          double *__restrict__ H, double *__restrict__ S,
+                                          double *__restrict__ part_b, double *__restrict__ part_k,
+                                          int *status, FusedSmem sm) {
+    using KL = KetLayout<N>;
+    constexpr int PS = Part<N>::size;
+    static_assert(PS <= 32, "the symmetric pass needs tri(n) + 1 + 3n <= 32");
+    const int lane = threadIdx.x & 31;
+    double *krow0 = sm.krow, *krow1 = sm.krow + 16 * 33, *kred = sm.kred;
+    const int k = tl.x * 32 + lane;
+    const int l0 = tl.y * LC;
+    const int l1 = min(l0 + LC, K);
+    const bool kval = k < K;
+    const double Ck = kval ? C[k] : 0.0;
+    SmemAcc<N> accH{sm.sacc + lane}, accS{sm.sacc + PS * 32 + lane};
+    accH.zero();
+    accS.zero();
+    // ket row output: lanes 2i and 2i+1 add their values; lane 2i writes row i
+    struct PairOut {
+        double *r;
+        bool lead;
+        __device__ __forceinline__ void put(int f, double v) {
+            v += __shfl_xor_sync(0xffffffffu, v, 1);
+            if (lead) r[f] = v;
+        }
+        __device__ __forceinline__ void add(int f, double v) {
+            v += __shfl_xor_sync(0xffffffffu, v, 1);
+            if (lead) r[f] += v;
+        }
+    } koH{krow0 + (lane >> 1) * 33, !(lane & 1)}, koS{krow1 + (lane >> 1) * 33, !(lane & 1)};
+    bool ok = true;
+    int flags = 0, bad = 0;
+    for (int l = l0; l < l1; ++l) {
+        double aH = 0.0, aS = 0.0, hsum = 0.0, ssum = 0.0;
+        const bool active = kval && l <= k;
+        const BraRef b{bra + (active ? k : l), (size_t)K};
+        for (int P = 0; P < nst; ++P) {
+            const double *kr = ket + ((size_t)l * nst + P) * KL::size;
+            const double wb = active ? kr[KL::wC] : 0.0;
+            const double wk = active && l < k ? 2.0 * Ck * kr[KL::winv] : 0.0;
+            double h, ov;
+            bool tok;
+            if constexpr (VKET)
+                tok = term_fused<N, double>(b, KetRefV{kr}, cs, wb, wk, accH, accS, koH, koS, h, ov);
+            else
+                tok = term_fused<N, double>(b, kr, cs, wb, wk, accH, accS, koH, koS, h, ov);
+            if (active) {
+                ok = tok && ok;
+                const double w = kr[KL::w];
+                hsum += w * h;
+                ssum += w * ov;
+            }
+            __syncwarp();
+#pragma unroll
+            for (int which = 0; which < 2; ++which) {
+                const double *kt = which ? krow1 : krow0;
+                double v = 0.0;
+                if (lane < PS)
+#pragma unroll
+                    for (int r = 0; r < 16; ++r) v += kt[r * 33 + lane];
+                kred[lane] = v;
+                __syncwarp();
+                if (lane < PS) {
+                    const double m = ket_map_apply(kmap, P, lane, PS, kred);
+                    if (which == 0) aH += m;
+                    else aS += m;
+                }
+                __syncwarp();
+            }
+        }
+        if (active) {
+            if (!isfinite(hsum) || !isfinite(ssum)) {
+                if (!(flags & 2)) bad = k * K + l;
+                flags |= 2;
+            }
+            H[(size_t)k * K + l] = hsum;
+            H[(size_t)l * K + k] = hsum;
+            S[(size_t)k * K + l] = ssum;
+            S[(size_t)l * K + k] = ssum;
+        }
+        if (lane < PS) {
+            part_k[(((size_t)t * LC + (l - l0)) * 2 + 0) * PS + lane] = aH;
+            part_k[(((size_t)t * LC + (l - l0)) * 2 + 1) * PS + lane] = aS;
+        }
+    }
+    if (kval) {
+#pragma unroll
+        for (int f = 0; f < 2 * PS; ++f) part_b[((size_t)t * 2 * PS + f) * 32 + lane] = sm.sacc[f * 32 + lane];
+    }
+    if (!ok) {
+        flags |= 1;
+        bad = k * K + l0;
+    }
+    flag_status(status, flags, bad);
+    __syncwarp();
+}
+
+// Sum of the fused-pass partials of basis m for field f: its bra partials from
+// the tiles of block kb = m / 32 (lane m % 32) and its ket partials from the
+// tiles of chunk lc = m / LC in every block kb' >= that chunk; returns
+// sum_H - E sum_S.
+template <int N>
+__device__ __forceinline__ double fsym_sum_one(const int *__restrict__ tstart, int LC, int K, int f, int m,
+                                               const double *__restrict__ part_b,
+                                               const double *__restrict__ part_k, double E) {
+    constexpr int PS = Part<N>::size;
+    const int kb = m >> 5, lane = m & 31;
+    double sH = 0.0, sS = 0.0;
+    for (int t = tstart[kb]; t < tstart[kb + 1]; ++t) {
+        sH += part_b[(((size_t)t * 2 + 0) * PS + f) * 32 + lane];
+        sS += part_b[(((size_t)t * 2 + 1) * PS + f) * 32 + lane];
+    }
+    const int lc = m / LC, ll = m - lc * LC;
+    const int nkb = (K + 31) >> 5;
+    int kb0 = lc * LC - 31;
+    kb0 = kb0 > 0 ? (kb0 + 31) >> 5 : 0;
+    for (int q = kb0; q < nkb; ++q) {
+        const size_t base = ((size_t)(tstart[q] + lc) * LC + ll) * 2;
+        sH += part_k[(base + 0) * PS + f];
+        sS += part_k[(base + 1) * PS + f];
+    }
+    return sH - E * sS;
+}
+
+}  // namespace necg

@@ -17,6 +17,7 @@
 #include <stdint.h>
 #include <math.h>
 
+#include "necg_device.cuh"
 #include "necg_kernels.cuh"
 #include "necg_lanes.cuh"
 #include "necg_math.cuh"
@@ -28,26 +29,6 @@ struct DevKet {
     const double *p;
     __device__ __forceinline__ const double *at(size_t off) const { return p + off; }
 };
-
-// Gradient accumulators of one lane in shared memory, interleaved by lane
-// (field t of lane j at t * 32 + j): conflict-free, and not held in registers.
-template <int N> struct SmemAcc {
-    double *p;  // shared base + lane
-    __device__ __forceinline__ void zero() {
-#pragma unroll
-        for (int t = 0; t < Part<N>::size; ++t) p[t * 32] = 0.0;
-    }
-    __device__ __forceinline__ double &g(int t) { return p[t * 32]; }
-    __device__ __forceinline__ double &d() { return p[tri(N) * 32]; }
-    __device__ __forceinline__ double &s(int t) { return p[(tri(N) + 1 + t) * 32]; }
-};
-
-// Status word: [0] bit flags, [1] first failing pair (row-major k*K + l).
-__device__ __forceinline__ void flag_status(int *status, int flags, int pair) {
-    if (!flags) return;
-    atomicOr(status, flags);
-    atomicMin(status + 1, pair);
-}
 
 template <int N>
 __global__ void __launch_bounds__(128) prep_bra_kernel(const double *__restrict__ iv, int K,
@@ -290,21 +271,9 @@ __global__ void __launch_bounds__(32, MINW) gsym_kernel(const int2 *__restrict__
     if (!ok) flag_status(status, 1, k * K + l0);
 }
 
-// Fused pass over unordered pairs (k >= l): the symmetric gradient pass of
-// gsym_kernel merged with the energy pass.  Each term gives the H element and
-// overlap (summed over P into H_kl = H_lk and S_kl = S_lk) and the bra and ket
-// gradients of h and of ov kept apart, since E is not known until finalize
-// has run on the H and S this pass writes; fsym_sum_kernel combines them as
-// g_H - E g_S.  Bra partials: part_b[((t * 2 + which) * PS + f) * 32 + lane];
-// ket partials: part_k[((t * LC + l - l0) * 2 + which) * PS + f], which = 0 for
-// H and 1 for S.
-//
-// Shared memory per warp must stay under 228 KB / 8 for 8 resident warps: the
-// ket rows of two lanes are added with one shuffle before they are written,
-// so each of the two ket tables has 16 rows.  The shuffles need the whole warp,
-// so every lane evaluates a term: a lane without a pair (l > k, or k >= K)
-// evaluates the finite pair (l, l, P) with zero weights, which adds nothing.
-template <int N, int MINW>
+// Fused pass over unordered pairs (k >= l): one warp per tile; the body is
+// fsym_tile (necg_device.cuh), shared with the batched persistent kernel.
+template <int N, int MINW, bool VKET>
 __global__ void __launch_bounds__(32, MINW) fsym_kernel(const int2 *__restrict__ tiles, int ntiles,
                                                    int LC, int K, int nst, Consts<N> cs,
                                                    const double *__restrict__ bra,
@@ -313,127 +282,27 @@ __global__ void __launch_bounds__(32, MINW) fsym_kernel(const int2 *__restrict__
                                                    double *__restrict__ H, double *__restrict__ S,
                                                    double *__restrict__ part_b,
                                                    double *__restrict__ part_k, int *status) {
-    using KL = KetLayout<N>;
-    constexpr int PS = Part<N>::size;
-    static_assert(PS <= 32, "the symmetric pass needs tri(n) + 1 + 3n <= 32");
-    __shared__ double sacc[2 * PS * 32];
-    __shared__ double krow[2][16 * 33];
+    __shared__ double sacc[2 * Part<N>::size * 32];
+    __shared__ double krow[2 * 16 * 33];
     __shared__ double kred[32];
     const int t = blockIdx.x;
-    const int lane = threadIdx.x;
     if (t >= ntiles) return;
-    const int2 tl = tiles[t];
-    const int k = tl.x * 32 + lane;
-    const int l0 = tl.y * LC;
-    const int l1 = min(l0 + LC, K);
-    const bool kval = k < K;
-    const double Ck = kval ? C[k] : 0.0;
-    SmemAcc<N> accH{sacc + lane}, accS{sacc + PS * 32 + lane};
-    accH.zero();
-    accS.zero();
-    // ket row output: lanes 2i and 2i+1 add their values; lane 2i writes row i
-    struct PairOut {
-        double *r;
-        bool lead;
-        __device__ __forceinline__ void put(int f, double v) {
-            v += __shfl_xor_sync(0xffffffffu, v, 1);
-            if (lead) r[f] = v;
-        }
-        __device__ __forceinline__ void add(int f, double v) {
-            v += __shfl_xor_sync(0xffffffffu, v, 1);
-            if (lead) r[f] += v;
-        }
-    } koH{krow[0] + (lane >> 1) * 33, !(lane & 1)}, koS{krow[1] + (lane >> 1) * 33, !(lane & 1)};
-    bool ok = true;
-    int flags = 0, bad = 0;
-    for (int l = l0; l < l1; ++l) {
-        double aH = 0.0, aS = 0.0, hsum = 0.0, ssum = 0.0;
-        const bool active = kval && l <= k;
-        const BraRef b{bra + (active ? k : l), (size_t)K};
-        for (int P = 0; P < nst; ++P) {
-            const double *kr = ket + ((size_t)l * nst + P) * KL::size;
-            const double wb = active ? kr[KL::wC] : 0.0;
-            const double wk = active && l < k ? 2.0 * Ck * kr[KL::winv] : 0.0;
-            double h, ov;
-            const bool tok = term_fused<N, double>(b, kr, cs, wb, wk, accH, accS, koH, koS, h, ov);
-            if (active) {
-                ok = tok && ok;
-                const double w = kr[KL::w];
-                hsum += w * h;
-                ssum += w * ov;
-            }
-            __syncwarp();
-#pragma unroll
-            for (int which = 0; which < 2; ++which) {
-                double v = 0.0;
-                if (lane < PS)
-#pragma unroll
-                    for (int r = 0; r < 16; ++r) v += krow[which][r * 33 + lane];
-                kred[lane] = v;
-                __syncwarp();
-                if (lane < PS) {
-                    const double m = ket_map_apply(kmap, P, lane, PS, kred);
-                    if (which == 0) aH += m;
-                    else aS += m;
-                }
-                __syncwarp();
-            }
-        }
-        if (active) {
-            if (!isfinite(hsum) || !isfinite(ssum)) {
-                if (!(flags & 2)) bad = k * K + l;
-                flags |= 2;
-            }
-            H[(size_t)k * K + l] = hsum;
-            H[(size_t)l * K + k] = hsum;
-            S[(size_t)k * K + l] = ssum;
-            S[(size_t)l * K + k] = ssum;
-        }
-        if (lane < PS) {
-            part_k[(((size_t)t * LC + (l - l0)) * 2 + 0) * PS + lane] = aH;
-            part_k[(((size_t)t * LC + (l - l0)) * 2 + 1) * PS + lane] = aS;
-        }
-    }
-    if (kval) {
-#pragma unroll
-        for (int f = 0; f < 2 * PS; ++f) part_b[((size_t)t * 2 * PS + f) * 32 + lane] = sacc[f * 32 + lane];
-    }
-    if (!ok) {
-        flags |= 1;
-        bad = k * K + l0;
-    }
-    flag_status(status, flags, bad);
+    fsym_tile<N, VKET>(t, tiles[t], LC, K, nst, cs, bra, ket, C, kmap, H, S, part_b, part_k, status,
+                       FusedSmem{sacc, krow, kred});
 }
 
-// Sum the fused-pass partials of basis m (the partial layout of gsym_sum_kernel,
-// doubled for H and S) and combine out[f * K + m] = sum_H - E sum_S with
-// E = scal[0], written by finalize after the pass.
+// Sum the fused-pass partials of basis m and combine out[f * K + m] =
+// sum_H - E sum_S with E = scal[0], written by finalize after the pass.
 template <int N>
 __global__ void __launch_bounds__(256) fsym_sum_kernel(const int *__restrict__ tstart, int LC, int K,
                                                        const double *__restrict__ part_b,
                                                        const double *__restrict__ part_k,
                                                        const double *__restrict__ scal,
                                                        double *__restrict__ out) {
-    constexpr int PS = Part<N>::size;
     const int id = blockIdx.x * blockDim.x + threadIdx.x;
-    if (id >= PS * K) return;
+    if (id >= Part<N>::size * K) return;
     const int f = id / K, m = id - f * K;
-    const int kb = m >> 5, lane = m & 31;
-    double sH = 0.0, sS = 0.0;
-    for (int t = tstart[kb]; t < tstart[kb + 1]; ++t) {
-        sH += part_b[(((size_t)t * 2 + 0) * PS + f) * 32 + lane];
-        sS += part_b[(((size_t)t * 2 + 1) * PS + f) * 32 + lane];
-    }
-    const int lc = m / LC, ll = m - lc * LC;
-    const int nkb = (K + 31) >> 5;
-    int kb0 = lc * LC - 31;
-    kb0 = kb0 > 0 ? (kb0 + 31) >> 5 : 0;
-    for (int q = kb0; q < nkb; ++q) {
-        const size_t base = ((size_t)(tstart[q] + lc) * LC + ll) * 2;
-        sH += part_k[(base + 0) * PS + f];
-        sS += part_k[(base + 1) * PS + f];
-    }
-    out[(size_t)f * K + m] = sH - scal[0] * sS;
+    out[(size_t)f * K + m] = fsym_sum_one<N>(tstart, LC, K, f, m, part_b, part_k, scal[0]);
 }
 
 // Sum the symmetric-pass partials of basis m into out[f * K + m]: its bra
@@ -764,19 +633,21 @@ template <int N> struct Launch {
                                                                       a.status);
         }
     }
-    template <int MINW> static void fsym_v(const LaunchArgs &a, cudaStream_t st) {
+    template <int MINW, bool VKET> static void fsym_v(const LaunchArgs &a, cudaStream_t st) {
         if constexpr (Part<N>::size <= 32) {
             Consts<N> cs = make_consts<N>(a.mass_h, a.ncv_h, a.efs);
-            fsym_kernel<N, MINW><<<a.nstiles, 32, 0, st>>>(
+            fsym_kernel<N, MINW, VKET><<<a.nstiles, 32, 0, st>>>(
                 a.stiles, a.nstiles, a.LC_s, a.K, a.nst, cs, a.bra, a.ket, a.C, a.kmap, a.H, a.S, a.psym,
                 a.psym + (size_t)a.nstiles * 2 * Part<N>::size * 32, a.status);
         }
     }
     static void fsym_tiles(const LaunchArgs &a, cudaStream_t st) {
-        switch (a.minb_s) {
-        case 12: fsym_v<12>(a, st); break;
-        case 16: fsym_v<16>(a, st); break;
-        default: fsym_v<8>(a, st); break;
+        switch (a.minb_s) {  // 100 + w: ket records read at the point of use
+        case 12: fsym_v<12, false>(a, st); break;
+        case 16: fsym_v<16, false>(a, st); break;
+        case 108: fsym_v<8, true>(a, st); break;
+        case 112: fsym_v<12, true>(a, st); break;
+        default: fsym_v<8, false>(a, st); break;
         }
     }
     static void fsym_reduce(const LaunchArgs &a, cudaStream_t st) {

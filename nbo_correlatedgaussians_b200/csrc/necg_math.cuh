@@ -132,6 +132,12 @@ struct BraRef {
     size_t K;
     __device__ __forceinline__ double operator()(int f) const { return ldv(p + (size_t)f * K); }
 };
+// Ket record read at the point of use (warp-uniform, L1 broadcast), so its
+// fields do not stay live in registers between their uses within a term.
+struct KetRefV {
+    const double *p;
+    __device__ __forceinline__ double operator[](int i) const { return ldv(p + i); }
+};
 #endif
 
 // Register accumulators of one bra gradient (see term_grad).
@@ -607,56 +613,39 @@ NECG_HD bool term_sym(const BA &b, const KA &kr, const Consts<N> &cs, R E, R wb,
             W[t] = ovk * (6.0 * b(BL::Nk + t) + W[t]) - fk * (b(BL::A + t) + kr[KL::Ap + t]);
         sandwich<N>(Bi, W, [&](int t, R v) { kout.put(t, v); });
     }
-    // Y = A_l' (T - S_l'), MY = M Y
+    // Y = A_l' (T - S_l'); Qk = Bi (Z' - 4 A_l' M Y); Ql = Bi (Z' + 4 A_k M Y) = Qk + 4 M Y
+    // (the difference of the two right-hand sides is 4 B M Y and Bi B = I)
     R Dl[3 * N], Y[3 * N];
 #pragma unroll
     for (int t = 0; t < 3 * N; ++t) Dl[t] = T[t] - kr[KL::Sp + t];
     symv3<N>(kr, KL::Ap, Dl, Y);
-    R Zl[3 * N];
-    {
-        R MY[3 * N];
 #pragma unroll
-        for (int i = 0; i < N; ++i)
+    for (int i = 0; i < N; ++i)
 #pragma unroll
-            for (int c = 0; c < 3; ++c) {
-                R s = cs.M[i * N] * Y[c];
+        for (int c = 0; c < 3; ++c) {
+            R s = kr[KL::AMp + i * N] * Y[c];
 #pragma unroll
-                for (int k = 1; k < N; ++k) s += cs.M[i * N + k] * Y[3 * k + c];
-                MY[3 * i + c] = s;
-            }
-        // Zl = Z' + 4 A_k (M Y) ; Z <- Zk = Z' - 4 (A_l' M) Y
-#pragma unroll
-        for (int i = 0; i < N; ++i)
-#pragma unroll
-            for (int c = 0; c < 3; ++c) {
-                R s = b(BL::A + sx(i, 0)) * MY[c];
-#pragma unroll
-                for (int k = 1; k < N; ++k) s += b(BL::A + sx(i, k)) * MY[3 * k + c];
-                Zl[3 * i + c] = Z[3 * i + c] + 4.0 * s;
-            }
-#pragma unroll
-        for (int i = 0; i < N; ++i)
-#pragma unroll
-            for (int c = 0; c < 3; ++c) {
-                R s = kr[KL::AMp + i * N] * Y[c];
-#pragma unroll
-                for (int k = 1; k < N; ++k) s += kr[KL::AMp + i * N + k] * Y[3 * k + c];
-                Z[3 * i + c] -= 4.0 * s;
-            }
-    }
+            for (int k = 1; k < N; ++k) s += kr[KL::AMp + i * N + k] * Y[3 * k + c];
+            Z[3 * i + c] -= 4.0 * s;
+        }
     R Qk[3 * N], Ql[3 * N];
 #pragma unroll
     for (int i = 0; i < N; ++i)
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-            R s = Bi[sx(i, 0)] * Z[c], t = Bi[sx(i, 0)] * Zl[c];
+            R s = Bi[sx(i, 0)] * Z[c];
 #pragma unroll
-            for (int k = 1; k < N; ++k) {
-                s += Bi[sx(i, k)] * Z[3 * k + c];
-                t += Bi[sx(i, k)] * Zl[3 * k + c];
-            }
+            for (int k = 1; k < N; ++k) s += Bi[sx(i, k)] * Z[3 * k + c];
             Qk[3 * i + c] = s;
-            Ql[3 * i + c] = t;
+        }
+#pragma unroll
+    for (int i = 0; i < N; ++i)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            R s = cs.M[i * N] * Y[c];
+#pragma unroll
+            for (int k = 1; k < N; ++k) s += cs.M[i * N + k] * Y[3 * k + c];
+            Ql[3 * i + c] = Qk[3 * i + c] + 4.0 * s;
         }
     // bra: acc.s += 2 ovb A_k Qk - 2 Fb Y ; ket: put 2 ovk A_l' Ql + 2 Fk Y
     {
@@ -751,54 +740,39 @@ NECG_HD bool term_fused(const BA &b, const KA &kr, const Consts<N> &cs, R wb, R 
             koS.put(t, -(sk * Bi[t]));
         }
     }
+    // Y = A_l' (T - S_l'); Qk = Bi (Z' - 4 A_l' M Y); Ql = Bi (Z' + 4 A_k M Y) = Qk + 4 M Y
+    // (the difference of the two right-hand sides is 4 B M Y and Bi B = I)
     R Dl[3 * N], Y[3 * N];
 #pragma unroll
     for (int t = 0; t < 3 * N; ++t) Dl[t] = T[t] - kr[KL::Sp + t];
     symv3<N>(kr, KL::Ap, Dl, Y);
-    R Zl[3 * N];
-    {
-        R MY[3 * N];
 #pragma unroll
-        for (int i = 0; i < N; ++i)
+    for (int i = 0; i < N; ++i)
 #pragma unroll
-            for (int c = 0; c < 3; ++c) {
-                R s = cs.M[i * N] * Y[c];
+        for (int c = 0; c < 3; ++c) {
+            R s = kr[KL::AMp + i * N] * Y[c];
 #pragma unroll
-                for (int k = 1; k < N; ++k) s += cs.M[i * N + k] * Y[3 * k + c];
-                MY[3 * i + c] = s;
-            }
-#pragma unroll
-        for (int i = 0; i < N; ++i)
-#pragma unroll
-            for (int c = 0; c < 3; ++c) {
-                R s = b(BL::A + sx(i, 0)) * MY[c];
-#pragma unroll
-                for (int k = 1; k < N; ++k) s += b(BL::A + sx(i, k)) * MY[3 * k + c];
-                Zl[3 * i + c] = Z[3 * i + c] + 4.0 * s;
-            }
-#pragma unroll
-        for (int i = 0; i < N; ++i)
-#pragma unroll
-            for (int c = 0; c < 3; ++c) {
-                R s = kr[KL::AMp + i * N] * Y[c];
-#pragma unroll
-                for (int k = 1; k < N; ++k) s += kr[KL::AMp + i * N + k] * Y[3 * k + c];
-                Z[3 * i + c] -= 4.0 * s;
-            }
-    }
+            for (int k = 1; k < N; ++k) s += kr[KL::AMp + i * N + k] * Y[3 * k + c];
+            Z[3 * i + c] -= 4.0 * s;
+        }
     R Qk[3 * N], Ql[3 * N];
 #pragma unroll
     for (int i = 0; i < N; ++i)
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-            R s = Bi[sx(i, 0)] * Z[c], t = Bi[sx(i, 0)] * Zl[c];
+            R s = Bi[sx(i, 0)] * Z[c];
 #pragma unroll
-            for (int k = 1; k < N; ++k) {
-                s += Bi[sx(i, k)] * Z[3 * k + c];
-                t += Bi[sx(i, k)] * Zl[3 * k + c];
-            }
+            for (int k = 1; k < N; ++k) s += Bi[sx(i, k)] * Z[3 * k + c];
             Qk[3 * i + c] = s;
-            Ql[3 * i + c] = t;
+        }
+#pragma unroll
+    for (int i = 0; i < N; ++i)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            R s = cs.M[i * N] * Y[c];
+#pragma unroll
+            for (int k = 1; k < N; ++k) s += cs.M[i * N + k] * Y[3 * k + c];
+            Ql[3 * i + c] = Qk[3 * i + c] + 4.0 * s;
         }
     // H: bra s += 2 ovb A_k Qk - 2 Fb Y, ket 2 ovk A_l' Ql + 2 Fk Y ; S: -2 ovb Y, +2 ovk Y
     {
