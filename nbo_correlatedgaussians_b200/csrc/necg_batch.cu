@@ -3,15 +3,18 @@
 // per-pair kernel a persistent launch that pulls (instance, tile) work items
 // from a flattened queue.
 //
-// Step sequence (fixed grids, so one captured CUDA graph serves any plan):
+// Step sequence (fixed grids, so one captured CUDA graph per mode serves any
+// plan).  Fused mode (every instance's symmetry set closed under inverse):
 //   reset        queue heads and per-instance status words
 //   prep         grid-stride over all (instance, k) bra and (instance, l, P) ket records
-//   energy       persistent warps over the energy tile queue (all instances)
+//   fused        persistent warps over the fused tile queue (all instances): H, S
+//                and the H and S gradient partials in one pass over unordered pairs
 //   rows         grid-stride warps over all (instance, row): (H C)_i, (S C)_i
 //   finalize     block per instance: E, norm, GRADC
-//   grad         persistent warps over the gradient tile queue
-//   sum          grid-stride over all (instance, field, k): sum the tile partials
+//   fsum         grid-stride over all (instance, field, k): g_H - E g_S
 //   reduce       grid-stride over all (instance, k): GRADA blocks
+// Ordered mode (any other set): energy tiles over the triangle and gradient
+// tiles over ordered pairs in place of fused, and a plain partial sum.
 // The plan (instance table, prefix sums, tile queues ordered by decreasing
 // cost) is built on the host and copied to device buffers before the step.
 #include <cuda_runtime.h>
@@ -21,6 +24,7 @@
 #include <algorithm>
 #include <vector>
 
+#include "necg_device.cuh"
 #include "necg_handle.h"
 #include "necg_lanes.cuh"
 #include "necg_math.cuh"
@@ -32,18 +36,23 @@ constexpr int kConstsDoubles = 72;  // >= sizeof(Consts<6>) / 8
 
 struct InstDesc {
     int n, K, nst, lc_e, lc_g, nlc;
-    int pad0, pad1;
+    int lc_s, nstiles;
     const double *iv, *C;
     double *bra, *ket, *part, *H, *S, *rows, *scal, *g, *f;
     const double *sml, *sms, *scvv;
     int *status;
+    // fused mode
+    const int *pinv, *stile_start;
+    double *psym;
+    KetMap kmap;
     double cs[kConstsDoubles];
 };
 
 struct PlanHdr {
     int ninst, ne, ng;
     int qe, qg;  // persistent queue heads
-    int pad[3];
+    int nf, qf;  // fused tile queue
+    int pad;
 };
 
 // plan buffer layout: [PlanHdr][InstDesc x cap][prefix arrays][tiles]
@@ -53,7 +62,7 @@ struct PlanPtrs {
     int *pref_bra;  // cumulative K            (ninst + 1)
     int *pref_ket;  // cumulative K * nst      (ninst + 1)
     int *pref_sum;  // cumulative PS * K       (ninst + 1)
-    int4 *etiles;   // (inst, kb, lc, 0)
+    int4 *etiles;   // (inst, kb, lc, 0); fused mode: (inst, kb, lc, tile index in the instance)
     int4 *gtiles;
 };
 
@@ -96,6 +105,7 @@ __global__ void batch_reset_kernel(PlanPtrs p) {
     if (threadIdx.x == 0) {
         p.hdr->qe = 0;
         p.hdr->qg = 0;
+        p.hdr->qf = 0;
     }
 }
 
@@ -114,7 +124,7 @@ __global__ void __launch_bounds__(128) batch_prep_kernel(PlanPtrs p) {
             const InstDesc &d = p.inst[q];
             const int id = j - p.pref_ket[q];
             BATCH_SWITCH(d.n, prep_ket_one<N>(d.iv, d.C, d.nst, consts_of<N>(d), d.sml, d.sms, d.scvv,
-                                             d.ket, id));
+                                             d.ket, id, d.pinv));
         }
     }
 }
@@ -142,6 +152,47 @@ __global__ void __launch_bounds__(32) batch_energy_kernel(PlanPtrs p) {
                                                            d.S, nullptr, nullptr, bad)));
             flag_inst(d.status, fl, bad);
         }
+    }
+}
+
+// Fused tiles of every instance: one warp per tile, pulled from the queue
+// (largest work first).  Shared memory is sized for n = 5; smaller n use a
+// prefix of it.
+__global__ void __launch_bounds__(32, 8) batch_fused_kernel(PlanPtrs p) {
+    __shared__ double sacc[2 * Part<kMaxN>::size * 32];
+    __shared__ double krow[2 * 16 * 33];
+    __shared__ double kred[32];
+    const int lane = threadIdx.x & 31;
+    const int nf = p.hdr->nf;
+    for (;;) {
+        int t = 0;
+        if (lane == 0) t = atomicAdd(&p.hdr->qf, 1);
+        t = __shfl_sync(0xffffffffu, t, 0);
+        if (t >= nf) break;
+        const int4 e = p.etiles[t];
+        const InstDesc &d = p.inst[e.x];
+        const size_t PSd = (size_t)(tri(d.n) + 1 + 3 * d.n);
+        double *part_b = d.psym, *part_k = d.psym + (size_t)d.nstiles * 2 * PSd * 32;
+        BATCH_SWITCH(d.n, (fsym_tile<N, true>(e.w, make_int2(e.y, e.z), d.lc_s, d.K, d.nst, consts_of<N>(d), d.bra,
+                                              d.ket, d.C, d.kmap, d.H, d.S, part_b, part_k, d.status,
+                                              FusedSmem{sacc, krow, kred})));
+    }
+}
+
+// g_H - E g_S of every instance into its part (field-major, chunk 0).
+__global__ void __launch_bounds__(256) batch_fsum_kernel(PlanPtrs p) {
+    const int ninst = p.hdr->ninst;
+    const int total = p.pref_sum[ninst];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+        const int q = find_inst(p.pref_sum, ninst, i);
+        const InstDesc &d = p.inst[q];
+        const int id = i - p.pref_sum[q];
+        const int f = id / d.K, m = id - f * d.K;
+        const size_t PSd = (size_t)(tri(d.n) + 1 + 3 * d.n);
+        const double *part_b = d.psym, *part_k = d.psym + (size_t)d.nstiles * 2 * PSd * 32;
+        double v = 0.0;
+        BATCH_SWITCH(d.n, v = fsym_sum_one<N>(d.stile_start, d.lc_s, d.K, f, m, part_b, part_k, d.scal[0]));
+        d.part[(size_t)f * d.K + m] = v;
     }
 }
 
@@ -292,14 +343,15 @@ using namespace necg;
 struct necg_batch {
     int cap_inst = 0, cap_tiles = 0;
     int device = 0, sms = 148;
-    int occ_energy = 8, occ_grad = 8;  // resident one-warp blocks per SM of the persistent kernels
+    int occ_energy = 8, occ_grad = 8, occ_fused = 8;  // resident one-warp blocks per SM (persistent kernels)
+    bool fused = false;  // mode of the current plan
     char *d_plan = nullptr;  // device plan buffer
     char *h_plan = nullptr;  // pinned host staging
     size_t plan_bytes = 0;
     PlanPtrs ptrs{};
     std::vector<necg_handle *> active;
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t exec = nullptr;
+    cudaGraph_t graph[2] = {};  // per mode: 0 ordered, 1 fused
+    cudaGraphExec_t exec[2] = {};
     cudaEvent_t uploaded = nullptr;  // recorded after the last plan upload from h_plan
     int ninst = 0, ne = 0, ng = 0;
 };
@@ -335,17 +387,41 @@ void layout(necg_batch *b, char *base, PlanPtrs &p, size_t *total) {
     if (total) *total = off;
 }
 
-void launch_step(necg_batch *b, cudaStream_t st) {
+void launch_step(necg_batch *b, cudaStream_t st, bool fused) {
     const PlanPtrs &p = b->ptrs;
     const int g = b->sms;
     batch_reset_kernel<<<1, 256, 0, st>>>(p);
     batch_prep_kernel<<<g * 4, 128, 0, st>>>(p);
-    batch_energy_kernel<<<g * b->occ_energy, 32, 0, st>>>(p);
-    batch_rows_kernel<<<g * 4, 256, 0, st>>>(p);
-    batch_finalize_kernel<<<g, 256, 0, st>>>(p);
-    batch_grad_kernel<<<g * b->occ_grad, 32, 0, st>>>(p);
-    batch_sum_kernel<<<g * 4, 256, 0, st>>>(p);
+    if (fused) {
+        batch_fused_kernel<<<g * b->occ_fused, 32, 0, st>>>(p);
+        batch_rows_kernel<<<g * 4, 256, 0, st>>>(p);
+        batch_finalize_kernel<<<g, 256, 0, st>>>(p);
+        batch_fsum_kernel<<<g * 4, 256, 0, st>>>(p);
+    } else {
+        batch_energy_kernel<<<g * b->occ_energy, 32, 0, st>>>(p);
+        batch_rows_kernel<<<g * 4, 256, 0, st>>>(p);
+        batch_finalize_kernel<<<g, 256, 0, st>>>(p);
+        batch_grad_kernel<<<g * b->occ_grad, 32, 0, st>>>(p);
+        batch_sum_kernel<<<g * 4, 256, 0, st>>>(p);
+    }
     batch_reduce_kernel<<<g * 2, 128, 0, st>>>(p);
+}
+
+int capture(necg_batch *b, int mode) {
+    if (b->exec[mode]) cudaGraphExecDestroy(b->exec[mode]);
+    if (b->graph[mode]) cudaGraphDestroy(b->graph[mode]);
+    b->exec[mode] = nullptr;
+    b->graph[mode] = nullptr;
+    cudaStream_t cap;
+    BCK(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+    cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+        launch_step(b, cap, mode == 1);
+        e = cudaStreamEndCapture(cap, &b->graph[mode]);
+    }
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&b->exec[mode], b->graph[mode], 0);
+    cudaStreamDestroy(cap);
+    return cfail(e);
 }
 }  // namespace
 
@@ -366,6 +442,9 @@ int necg_batch_create(int max_instances, int max_tiles, necg_batch **out) {
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b->occ_grad, batch_grad_kernel, 32, 0) != cudaSuccess ||
         b->occ_grad < 1)
         b->occ_grad = 8;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b->occ_fused, batch_fused_kernel, 32, 0) != cudaSuccess ||
+        b->occ_fused < 1)
+        b->occ_fused = 8;
     PlanPtrs tmp{};
     layout(b, nullptr, tmp, &b->plan_bytes);
     cudaError_t e = cudaMalloc((void **)&b->d_plan, b->plan_bytes);
@@ -385,8 +464,10 @@ int necg_batch_create(int max_instances, int max_tiles, necg_batch **out) {
 int necg_batch_destroy(necg_batch *b) {
     if (!b) return NECG_ERR_ARG;
     cudaSetDevice(b->device);
-    if (b->exec) cudaGraphExecDestroy(b->exec);
-    if (b->graph) cudaGraphDestroy(b->graph);
+    for (int m = 0; m < 2; ++m) {
+        if (b->exec[m]) cudaGraphExecDestroy(b->exec[m]);
+        if (b->graph[m]) cudaGraphDestroy(b->graph[m]);
+    }
     if (b->uploaded) cudaEventDestroy(b->uploaded);
     cudaFree(b->d_plan);
     cudaFreeHost(b->h_plan);
@@ -411,6 +492,10 @@ int necg_batch_plan(necg_batch *b, int count, necg_handle *const *hs, const int 
     };
     std::vector<Cost> et, gt;
     hp.pref_bra[0] = hp.pref_ket[0] = hp.pref_sum[0] = 0;
+    bool fused = count > 0;
+    for (int q = 0; q < count; ++q) {
+        if (!hs[q] || !hs[q]->sym_ok || hs[q]->n > kMaxN) fused = false;
+    }
     for (int q = 0; q < count; ++q) {
         necg_handle *h = hs[q];
         const int K = Ks[q];
@@ -442,12 +527,32 @@ int necg_batch_plan(necg_batch *b, int count, necg_handle *const *hs, const int 
         d.scvv = h->d_scvv;
         d.status = h->d_status;
         BATCH_SWITCH(n, fill_consts<N>(d, h));
+        if (fused) {
+            int rc = prepare_fused(h, K, st);
+            if (rc) return rc;
+            d.lc_s = h->lc_s;
+            d.nstiles = h->nstiles;
+            d.pinv = h->d_pinv;
+            d.stile_start = h->d_stile_start;
+            d.psym = h->d_psym;
+            d.kmap = KetMap{h->d_kcnt, h->d_ksrc, h->d_kcoef, h->kmaxnz};
+        }
         const int ps = tri(n) + 1 + 3 * n;
         hp.pref_bra[q + 1] = hp.pref_bra[q] + K;
         hp.pref_ket[q + 1] = hp.pref_ket[q] + K * h->nst;
         hp.pref_sum[q + 1] = hp.pref_sum[q] + ps * K;
-        const long long fe = necg_term_flops(n, 0, nullptr), fg = necg_term_flops(n, 1, nullptr);
         const int nkb = (K + 31) / 32;
+        if (fused) {  // the instance's own tile numbering (the partial layout depends on it)
+            const double ff = (double)necg_term_flops(n, 3, nullptr) * h->nst * d.lc_s;
+            int t = 0;
+            for (int kb = 0; kb < nkb; ++kb) {
+                const int last = kb * 32 + 31 < K - 1 ? kb * 32 + 31 : K - 1;
+                for (int lc = 0; lc <= last / d.lc_s; ++lc, ++t) et.push_back({ff, make_int4(q, kb, lc, t)});
+            }
+            if (t != d.nstiles) return NECG_ERR_ARG;
+            continue;
+        }
+        const long long fe = necg_term_flops(n, 0, nullptr), fg = necg_term_flops(n, 1, nullptr);
         for (int kb = 0; kb < nkb; ++kb)
             for (int lc = 0; lc * d.lc_e <= kb * 32 + 31 && lc * d.lc_e < K; ++lc)
                 et.push_back({(double)fe * h->nst * d.lc_e, make_int4(q, kb, lc, 0)});
@@ -462,14 +567,23 @@ int necg_batch_plan(necg_batch *b, int count, necg_handle *const *hs, const int 
     for (size_t i = 0; i < et.size(); ++i) hp.etiles[i] = et[i].t;
     for (size_t i = 0; i < gt.size(); ++i) hp.gtiles[i] = gt[i].t;
     hp.hdr->ninst = count;
-    hp.hdr->ne = (int)et.size();
+    hp.hdr->ne = fused ? 0 : (int)et.size();
     hp.hdr->ng = (int)gt.size();
-    hp.hdr->qe = hp.hdr->qg = 0;
+    hp.hdr->nf = fused ? (int)et.size() : 0;
+    hp.hdr->qe = hp.hdr->qg = hp.hdr->qf = 0;
+    b->fused = fused;
     b->ninst = count;
     b->ne = (int)et.size();
     b->ng = (int)gt.size();
     b->active.assign(hs, hs + count);
-    BCK(cudaMemcpyAsync(b->d_plan, b->h_plan, b->plan_bytes, cudaMemcpyHostToDevice, st));
+    // upload only what this plan uses: header, instance table and prefixes,
+    // then the used part of each tile queue
+    const size_t head = (size_t)((char *)hp.etiles - b->h_plan);
+    const size_t off_g = (size_t)((char *)hp.gtiles - b->h_plan);
+    BCK(cudaMemcpyAsync(b->d_plan, b->h_plan, head + et.size() * sizeof(int4), cudaMemcpyHostToDevice, st));
+    if (!gt.empty())
+        BCK(cudaMemcpyAsync(b->d_plan + off_g, b->h_plan + off_g, gt.size() * sizeof(int4),
+                            cudaMemcpyHostToDevice, st));
     if (!b->uploaded) BCK(cudaEventCreateWithFlags(&b->uploaded, cudaEventDisableTiming));
     BCK(cudaEventRecord(b->uploaded, st));
     return NECG_OK;
@@ -478,39 +592,26 @@ int necg_batch_plan(necg_batch *b, int count, necg_handle *const *hs, const int 
 int necg_batch_step(necg_batch *b, void *stream) {
     if (!b) return NECG_ERR_ARG;
     BCK(cudaSetDevice(b->device));
-    launch_step(b, (cudaStream_t)stream);
+    launch_step(b, (cudaStream_t)stream, b->fused);
     return cfail(cudaGetLastError());
 }
 
 int necg_batch_graph(necg_batch *b, void *stream) {
     if (!b) return NECG_ERR_ARG;
     BCK(cudaSetDevice(b->device));
-    cudaStream_t st = (cudaStream_t)stream;
-    if (b->exec) {
-        cudaGraphExecDestroy(b->exec);
-        b->exec = nullptr;
-    }
-    if (b->graph) {
-        cudaGraphDestroy(b->graph);
-        b->graph = nullptr;
-    }
-    cudaStream_t cap;
-    BCK(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
-    cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
-    if (e == cudaSuccess) {
-        launch_step(b, cap);
-        e = cudaStreamEndCapture(cap, &b->graph);
-    }
-    if (e == cudaSuccess) e = cudaGraphInstantiate(&b->exec, b->graph, 0);
-    cudaStreamDestroy(cap);
-    (void)st;
-    return cfail(e);
+    (void)stream;
+    return capture(b, b->fused ? 1 : 0);
 }
 
 int necg_batch_replay(necg_batch *b, void *stream) {
-    if (!b || !b->exec) return NECG_ERR_ARG;
+    if (!b) return NECG_ERR_ARG;
     BCK(cudaSetDevice(b->device));
-    BCK(cudaGraphLaunch(b->exec, (cudaStream_t)stream));
+    const int mode = b->fused ? 1 : 0;
+    if (!b->exec[mode]) {  // the graph of this plan's mode was not captured yet
+        int rc = capture(b, mode);
+        if (rc) return rc;
+    }
+    BCK(cudaGraphLaunch(b->exec[mode], (cudaStream_t)stream));
     return NECG_OK;
 }
 

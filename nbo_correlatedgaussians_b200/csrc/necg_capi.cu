@@ -89,9 +89,9 @@ int ensure_tiles(necg_handle *h, int K, cudaStream_t st) {
 
 // Lower-triangle tiles of chunk LC for the symmetric pass, plus the first tile
 // of each 32-row block; the partial buffer grows here if this K and LC need more.
-int ensure_sym_tiles(necg_handle *h, int K, cudaStream_t st) {
+// mult = 2 for the fused pass (H and S partials kept apart), 1 otherwise.
+int ensure_sym_tiles(necg_handle *h, int K, cudaStream_t st, int mult) {
     const int PS = necg::part_stride(h->n);
-    const size_t mult = h->grad_mode == 2 ? 2 : 1;  // the fused pass keeps H and S partials apart
     if (h->stiles_K == K && h->stiles_lc == h->lc_s &&
         (size_t)h->nstiles * PS * (32 + h->lc_s) * mult <= h->psym_cap)
         return NECG_OK;
@@ -127,6 +127,16 @@ int ensure_sym_tiles(necg_handle *h, int K, cudaStream_t st) {
     h->nstiles = (int)t.size();
     return NECG_OK;
 }
+
+}  // namespace
+
+int necg::prepare_fused(necg_handle *h, int K, cudaStream_t st) {
+    if (!h || !h->sym_ok) return NECG_ERR_UNSUPPORTED;
+    CK(cudaSetDevice(h->device));
+    return ensure_sym_tiles(h, K, st, 2);
+}
+
+namespace {
 
 // Inverse of each symmetry term (sml and sms both inverted) and the map of a
 // ket gradient from P's frame to the basis function's frame.  Sets sym_ok
@@ -244,7 +254,7 @@ LaunchArgs base_args(necg_handle *h, int K) {
 // symmetric pass alone is used.)
 int launch_gradient(necg_handle *h, LaunchArgs &a, cudaStream_t st) {
     if (h->grad_mode >= 1) {
-        int rc = ensure_sym_tiles(h, a.K, st);
+        int rc = ensure_sym_tiles(h, a.K, st, h->grad_mode == 2 ? 2 : 1);
         if (rc) return rc;
         a.stiles = h->d_stiles;
         a.stile_start = h->d_stile_start;
@@ -416,7 +426,7 @@ int necg_outprod(necg_handle *h, int K, const double *x_dev, double *f_dev, doub
     a.H = H_dev ? H_dev : h->d_H;
     a.S = S_dev ? S_dev : h->d_S;
     a.g = g_dev;
-    if (h->grad_mode >= 1 && (rc = ensure_sym_tiles(h, K, st))) return rc;
+    if (h->grad_mode >= 1 && (rc = ensure_sym_tiles(h, K, st, h->grad_mode == 2 ? 2 : 1))) return rc;
     if (h->grad_mode == 2) {
         // fused: one pass over unordered pairs writes H, S and the split gradients
         a.stiles = h->d_stiles;

@@ -39,3 +39,10 @@ struct necg_handle {
     double *d_psym = nullptr;
     size_t psym_cap = 0;  // doubles
 };
+
+namespace necg {
+// Tile list and partial buffers of the fused pass for bases of K functions
+// (the handle's ket chunk lc_s), as the batched step needs them; returns a
+// status code.  May synchronise `st` when the list changes.
+int prepare_fused(necg_handle *h, int K, cudaStream_t st);
+}  // namespace necg

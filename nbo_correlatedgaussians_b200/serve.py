@@ -81,9 +81,10 @@ class Request:
 
 class Server:
     def __init__(self, budget_bytes: float = 120e9, max_slots: int = 256, graph: bool = True, tune: bool = True,
-                 device=None):
+                 device=None, max_tiles: int = 1 << 22):
         self.budget = float(budget_bytes)
         self.max_slots = int(max_slots)
+        self.max_tiles = int(max_tiles)  # tiles of one step (all runs); 16 bytes each per queue
         self.graph = graph
         self.tune = tune
         self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
@@ -106,7 +107,7 @@ class Server:
     # ----------------------------------------------------------- lifecycle
     def start(self) -> "Server":
         self.stream = torch.cuda.Stream(device=self.device)
-        self.batches = [Batch(self.max_slots), Batch(self.max_slots)]
+        self.batches = [Batch(self.max_slots, self.max_tiles), Batch(self.max_slots, self.max_tiles)]
         self.t_start = time.perf_counter()
         self._thread = threading.Thread(target=self._loop, name="necg-server", daemon=True)
         self._thread.start()

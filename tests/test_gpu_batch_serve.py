@@ -109,6 +109,36 @@ def test_batch_matches_single_and_is_order_independent(torch_cuda):
         assert fi == res[i][0] and np.array_equal(gi, res[i][1])
 
 
+def test_batch_modes_fused_and_ordered(torch_cuda):
+    """A plan whose instances all have symmetry sets closed under inverse runs
+    the fused step; adding one instance without that property switches the
+    whole plan to the ordered step (and its own CUDA graph).  Both against the
+    oracle, and the fused results are bitwise the same before and after."""
+    from nbo_correlatedgaussians_b200 import synth
+    from nbo_correlatedgaussians_b200.batch import BatchEngine
+    probs = _mixed(30)
+    r = synth.make_problem("H2", 24, 31)  # a lone non-involutory map: no inverse in the set
+    M = np.array([[1.0, 0, 0], [0, 0, 1.0], [0, 1.0, 0]]) @ np.array([[1.0, 0, 0], [1.0, 1.0, 0], [0, 0, 1.0]])
+    r.sml = np.stack([np.eye(3), M])
+    r.sms = np.stack([np.eye(9), np.kron(np.linalg.inv(M), np.eye(3))])
+    r.scvv = np.array([0.5, 0.5])
+    be = BatchEngine(probs + [r], tune=False)
+    res = {}
+    for active in (list(range(len(probs))), list(range(len(probs) + 1)), list(range(len(probs)))):
+        be.plan(active)
+        be.step(graph=True)
+        be.check()
+        for i in active:
+            p = (probs + [r])[i]
+            f, g = be.results(i)
+            fo, go = Oracle.from_problem(p).outprod(p.x, nthreads=8)
+            assert abs(f - fo) < TOL_E and normwise(g, go) < TOL_G
+            if len(active) == len(probs):
+                if i in res:
+                    assert f == res[i][0] and np.array_equal(g, res[i][1])
+                res[i] = (f, g)
+
+
 def test_batch_graph_replay_tracks_new_inputs(torch_cuda):
     from nbo_correlatedgaussians_b200.batch import BatchEngine
     probs = _mixed(10)
