@@ -98,6 +98,30 @@ int necg_outprod(necg_handle *h, int K, const double *x_dev, double *f_dev, doub
 int necg_outprod_host(necg_handle *h, int K, const double *x_host, double *f_host,
                       double *g_host, void *stream);
 
+/* One evaluation split across ranks (one process per GPU): the replacement of
+ * the row-cyclic MPI split of source/outprod.f90:34-45 and
+ * source/make_grad.f90:16-90 and its two MPI_REDUCE calls.  Each rank takes a
+ * contiguous range [tile_begin, tile_end) of the fused pass's tiles (count from
+ * necg_shard_tiles; same on every rank for the same handle settings):
+ *   necg_shard_pairs   its tiles' H and S entries and gradient partials;
+ *                      rows_dev (2K) = this shard's (H C, S C)
+ *   -- the caller sums rows_dev over the ranks (all-reduce, 2K doubles) --
+ *   necg_shard_grad    E, norm, GRADC from the summed rows (f_dev, g_dev);
+ *                      sums_dev (part_stride(n) * K) = this shard's per-basis
+ *                      gradient sums g_H - E g_S
+ *   -- the caller sums sums_dev over the ranks (all-reduce) --
+ *   necg_shard_finish  GRADA from the summed sums into g_dev
+ * Every rank ends with the full f and g.  Needs the symmetry set closed under
+ * inverse (NECG_ERR_UNSUPPORTED otherwise).  The three calls are one
+ * evaluation: on one handle they must not interleave with other calls. */
+int necg_shard_tiles(necg_handle *h, int K, int *ntiles);
+int necg_shard_pairs(necg_handle *h, int K, const double *x_dev, int tile_begin, int tile_end,
+                     double *rows_dev, void *stream);
+int necg_shard_grad(necg_handle *h, int K, const double *x_dev, const double *rows_dev, int tile_begin,
+                    int tile_end, double *f_dev, double *g_dev, double *sums_dev, void *stream);
+int necg_shard_finish(necg_handle *h, int K, const double *x_dev, const double *sums_dev, double *g_dev,
+                      void *stream);
+
 /* Energy only: H, S (and optionally the kinetic and Coulomb parts Kin, Pot,
  * NULL to skip); when C_dev and en_dev are non-NULL, en_dev[0..1] receive
  * E = C^T H C / C^T S C and norm = 1 / C^T S C.

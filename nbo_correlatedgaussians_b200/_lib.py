@@ -41,6 +41,10 @@ SIGNATURES = [
     ("necg_matel", _i, [_vp, _i, _vp, _i, _vp, _vp, _vp]),
     ("necg_gradel", _i, [_vp, _i, _vp, _i, _vp, _vp, _vp, _vp]),
     ("necg_rrms", _i, [_vp, _i, _vp, _i, _vp, _vp, _vp]),
+    ("necg_shard_tiles", _i, [_vp, _i, _vp]),
+    ("necg_shard_pairs", _i, [_vp, _i, _vp, _i, _i, _vp, _vp]),
+    ("necg_shard_grad", _i, [_vp, _i, _vp, _vp, _i, _i, _vp, _vp, _vp, _vp]),
+    ("necg_shard_finish", _i, [_vp, _i, _vp, _vp, _vp, _vp]),
     ("necg_dipole", _i, [_vp, _i, _vp, _vp, _vp, _vp, _vp]),
     ("necg_f0", _i, [_vp, _i, _vp, _vp, _vp]),
     ("necg_outprod_noalloc", _i, [_i, _i, _i, _d, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),

@@ -43,6 +43,7 @@ struct InstDesc {
     int *status;
     // fused mode
     const int *pinv, *stile_start;
+    const int2 *stiles;  // the instance's fused tile list (kb, lc), on the device
     double *psym;
     KetMap kmap;
     double cs[kConstsDoubles];
@@ -62,6 +63,8 @@ struct PlanPtrs {
     int *pref_bra;  // cumulative K            (ninst + 1)
     int *pref_ket;  // cumulative K * nst      (ninst + 1)
     int *pref_sum;  // cumulative PS * K       (ninst + 1)
+    int *pref_ft;   // cumulative fused tiles  (ninst + 1) over the instances in `order`
+    int *order;     // instances by decreasing tile cost (fused queue order)
     int4 *etiles;   // (inst, kb, lc, 0); fused mode: (inst, kb, lc, tile index in the instance)
     int4 *gtiles;
 };
@@ -155,9 +158,10 @@ __global__ void __launch_bounds__(32) batch_energy_kernel(PlanPtrs p) {
     }
 }
 
-// Fused tiles of every instance: one warp per tile, pulled from the queue
-// (largest work first).  Shared memory is sized for n = 5; smaller n use a
-// prefix of it.
+// Fused tiles of every instance: one warp per tile, pulled from one queue
+// that runs over the instances in plan order (largest tiles first) and over
+// each instance's own device tile list.  Shared memory is sized for n = 5;
+// smaller n use a prefix of it.
 __global__ void __launch_bounds__(32, 8) batch_fused_kernel(PlanPtrs p) {
     __shared__ double sacc[2 * Part<kMaxN>::size * 32];
     __shared__ double krow[2 * 16 * 33];
@@ -169,11 +173,12 @@ __global__ void __launch_bounds__(32, 8) batch_fused_kernel(PlanPtrs p) {
         if (lane == 0) t = atomicAdd(&p.hdr->qf, 1);
         t = __shfl_sync(0xffffffffu, t, 0);
         if (t >= nf) break;
-        const int4 e = p.etiles[t];
-        const InstDesc &d = p.inst[e.x];
+        const int j = find_inst(p.pref_ft, p.hdr->ninst, t);
+        const InstDesc &d = p.inst[p.order[j]];
+        const int ti = t - p.pref_ft[j];  // tile index within the instance
         const size_t PSd = (size_t)(tri(d.n) + 1 + 3 * d.n);
         double *part_b = d.psym, *part_k = d.psym + (size_t)d.nstiles * 2 * PSd * 32;
-        BATCH_SWITCH(d.n, (fsym_tile<N, true>(e.w, make_int2(e.y, e.z), d.lc_s, d.K, d.nst, consts_of<N>(d), d.bra,
+        BATCH_SWITCH(d.n, (fsym_tile<N, true>(ti, d.stiles[ti], d.lc_s, d.K, d.nst, consts_of<N>(d), d.bra,
                                               d.ket, d.C, d.kmap, d.H, d.S, part_b, part_k, d.status,
                                               FusedSmem{sacc, krow, kred})));
     }
@@ -380,6 +385,10 @@ void layout(necg_batch *b, char *base, PlanPtrs &p, size_t *total) {
     off = align_up(off + sizeof(int) * (b->cap_inst + 1), 256);
     p.pref_sum = (int *)(base + off);
     off = align_up(off + sizeof(int) * (b->cap_inst + 1), 256);
+    p.pref_ft = (int *)(base + off);
+    off = align_up(off + sizeof(int) * (b->cap_inst + 1), 256);
+    p.order = (int *)(base + off);
+    off = align_up(off + sizeof(int) * (b->cap_inst + 1), 256);
     p.etiles = (int4 *)(base + off);
     off = align_up(off + sizeof(int4) * b->cap_tiles, 256);
     p.gtiles = (int4 *)(base + off);
@@ -491,6 +500,12 @@ int necg_batch_plan(necg_batch *b, int count, necg_handle *const *hs, const int 
         int4 t;
     };
     std::vector<Cost> et, gt;
+    std::vector<double> fcost(count > 0 ? count : 1, 0.0);
+    static const std::vector<long long> flops_fused = [] {
+        std::vector<long long> v(kMaxN + 1, 0);
+        for (int n = 1; n <= kMaxN; ++n) v[n] = necg_term_flops(n, 3, nullptr);
+        return v;
+    }();
     hp.pref_bra[0] = hp.pref_ket[0] = hp.pref_sum[0] = 0;
     bool fused = count > 0;
     for (int q = 0; q < count; ++q) {
@@ -536,20 +551,15 @@ int necg_batch_plan(necg_batch *b, int count, necg_handle *const *hs, const int 
             d.stile_start = h->d_stile_start;
             d.psym = h->d_psym;
             d.kmap = KetMap{h->d_kcnt, h->d_ksrc, h->d_kcoef, h->kmaxnz};
+            d.stiles = h->d_stiles;
         }
         const int ps = tri(n) + 1 + 3 * n;
         hp.pref_bra[q + 1] = hp.pref_bra[q] + K;
         hp.pref_ket[q + 1] = hp.pref_ket[q] + K * h->nst;
         hp.pref_sum[q + 1] = hp.pref_sum[q] + ps * K;
         const int nkb = (K + 31) / 32;
-        if (fused) {  // the instance's own tile numbering (the partial layout depends on it)
-            const double ff = (double)necg_term_flops(n, 3, nullptr) * h->nst * d.lc_s;
-            int t = 0;
-            for (int kb = 0; kb < nkb; ++kb) {
-                const int last = kb * 32 + 31 < K - 1 ? kb * 32 + 31 : K - 1;
-                for (int lc = 0; lc <= last / d.lc_s; ++lc, ++t) et.push_back({ff, make_int4(q, kb, lc, t)});
-            }
-            if (t != d.nstiles) return NECG_ERR_ARG;
+        if (fused) {  // tiles come from the instance's device list; only its cost is needed here
+            fcost[q] = (double)flops_fused[n] * h->nst * d.lc_s;
             continue;
         }
         const long long fe = necg_term_flops(n, 0, nullptr), fg = necg_term_flops(n, 1, nullptr);
@@ -560,6 +570,17 @@ int necg_batch_plan(necg_batch *b, int count, necg_handle *const *hs, const int 
             for (int kb = 0; kb < nkb; ++kb)
                 gt.push_back({(double)fg * h->nst * d.lc_g, make_int4(q, kb, lc, 0)});
     }
+    long long nf = 0;
+    if (fused) {  // fused queue: instances by decreasing tile cost, each over its own tile list
+        for (int q = 0; q < count; ++q) hp.order[q] = q;
+        std::stable_sort(hp.order, hp.order + count, [&](int a, int c) { return fcost[a] > fcost[c]; });
+        hp.pref_ft[0] = 0;
+        for (int j = 0; j < count; ++j) {
+            nf += hp.inst[hp.order[j]].nstiles;
+            if (nf > 0x7fffffff) return NECG_ERR_CAPACITY;
+            hp.pref_ft[j + 1] = (int)nf;
+        }
+    }
     if ((int)et.size() > b->cap_tiles || (int)gt.size() > b->cap_tiles) return NECG_ERR_CAPACITY;
     auto by_cost = [](const Cost &a, const Cost &c) { return a.c > c.c; };
     std::stable_sort(et.begin(), et.end(), by_cost);
@@ -569,7 +590,7 @@ int necg_batch_plan(necg_batch *b, int count, necg_handle *const *hs, const int 
     hp.hdr->ninst = count;
     hp.hdr->ne = fused ? 0 : (int)et.size();
     hp.hdr->ng = (int)gt.size();
-    hp.hdr->nf = fused ? (int)et.size() : 0;
+    hp.hdr->nf = fused ? (int)nf : 0;
     hp.hdr->qe = hp.hdr->qg = hp.hdr->qf = 0;
     b->fused = fused;
     b->ninst = count;

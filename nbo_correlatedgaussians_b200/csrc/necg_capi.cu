@@ -456,6 +456,92 @@ int necg_outprod(necg_handle *h, int K, const double *x_dev, double *f_dev, doub
     return finish_launch();
 }
 
+// ---- one evaluation split across ranks (tiles of the fused pass) -----------
+namespace {
+int shard_args(necg_handle *h, int K, const double *x_dev, int t0, int t1, cudaStream_t st, LaunchArgs &a) {
+    int rc = check_K(h, K);
+    if (rc) return rc;
+    if (!x_dev) return NECG_ERR_ARG;
+    if (!h->sym_ok) return NECG_ERR_UNSUPPORTED;
+    CK(cudaSetDevice(h->device));
+    if ((rc = ensure_sym_tiles(h, K, st, 2))) return rc;
+    if (t0 < 0 || t1 < t0 || t1 > h->nstiles) return NECG_ERR_ARG;
+    a = base_args(h, K);
+    const size_t siv = (size_t)K * (h->n * (h->n + 1) / 2 + 3 * h->n);
+    a.iv = x_dev;
+    a.C = x_dev + siv;
+    a.stiles = h->d_stiles;
+    a.stile_start = h->d_stile_start;
+    a.nstiles = h->nstiles;
+    a.LC_s = h->lc_s;
+    a.psym = h->d_psym;
+    a.st_begin = t0;
+    a.st_end = t1;
+    return NECG_OK;
+}
+}  // namespace
+
+int necg_shard_tiles(necg_handle *h, int K, int *ntiles) {
+    if (!ntiles) return NECG_ERR_ARG;
+    int rc = check_K(h, K);
+    if (rc) return rc;
+    if (!h->sym_ok) return NECG_ERR_UNSUPPORTED;
+    CK(cudaSetDevice(h->device));
+    if ((rc = ensure_sym_tiles(h, K, h->last_stream, 2))) return rc;
+    *ntiles = h->nstiles;
+    return NECG_OK;
+}
+
+int necg_shard_pairs(necg_handle *h, int K, const double *x_dev, int tile_begin, int tile_end,
+                     double *rows_dev, void *stream) {
+    cudaStream_t st = (cudaStream_t)stream;
+    LaunchArgs a;
+    int rc = shard_args(h, K, x_dev, tile_begin, tile_end, st, a);
+    if (rc) return rc;
+    if (!rows_dev) return NECG_ERR_ARG;
+    if ((rc = begin(h, st))) return rc;
+    // this shard writes only its tiles' entries of H and S: the rest must be 0
+    CK(cudaMemsetAsync(h->d_H, 0, sizeof(double) * (size_t)K * K, st));
+    CK(cudaMemsetAsync(h->d_S, 0, sizeof(double) * (size_t)K * K, st));
+    if (necg::launch_prep(a, st)) return NECG_ERR_UNSUPPORTED;
+    if (tile_end > tile_begin) necg::launch_fsym(a, st);
+    necg::launch_rows(a, rows_dev, st);
+    return finish_launch();
+}
+
+int necg_shard_grad(necg_handle *h, int K, const double *x_dev, const double *rows_dev, int tile_begin,
+                    int tile_end, double *f_dev, double *g_dev, double *sums_dev, void *stream) {
+    cudaStream_t st = (cudaStream_t)stream;
+    LaunchArgs a;
+    int rc = shard_args(h, K, x_dev, tile_begin, tile_end, st, a);
+    if (rc) return rc;
+    if (!rows_dev || !g_dev || !sums_dev) return NECG_ERR_ARG;
+    h->last_stream = st;
+    const size_t siv = (size_t)K * (h->n * (h->n + 1) / 2 + 3 * h->n);
+    a.g = g_dev;
+    a.sums = sums_dev;
+    necg::launch_finalize(a, rows_dev, f_dev, g_dev + siv, st);
+    necg::launch_fsym_reduce(a, st);  // per-basis sums of this shard's tiles only
+    return finish_launch();
+}
+
+int necg_shard_finish(necg_handle *h, int K, const double *x_dev, const double *sums_dev, double *g_dev,
+                      void *stream) {
+    int rc = check_K(h, K);
+    if (rc) return rc;
+    if (!x_dev || !sums_dev || !g_dev) return NECG_ERR_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    CK(cudaSetDevice(h->device));
+    h->last_stream = st;
+    LaunchArgs a = base_args(h, K);
+    const size_t siv = (size_t)K * (h->n * (h->n + 1) / 2 + 3 * h->n);
+    a.iv = x_dev;
+    a.C = x_dev + siv;
+    a.g = g_dev;
+    necg::launch_reduce_sums(a, sums_dev, st);
+    return finish_launch();
+}
+
 int necg_outprod_host(necg_handle *h, int K, const double *x_host, double *f_host,
                       double *g_host, void *stream) {
     int rc = check_K(h, K);

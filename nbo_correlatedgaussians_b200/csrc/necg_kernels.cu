@@ -274,7 +274,7 @@ __global__ void __launch_bounds__(32, MINW) gsym_kernel(const int2 *__restrict__
 // Fused pass over unordered pairs (k >= l): one warp per tile; the body is
 // fsym_tile (necg_device.cuh), shared with the batched persistent kernel.
 template <int N, int MINW, bool VKET>
-__global__ void __launch_bounds__(32, MINW) fsym_kernel(const int2 *__restrict__ tiles, int ntiles,
+__global__ void __launch_bounds__(32, MINW) fsym_kernel(const int2 *__restrict__ tiles, int t_begin, int t_end,
                                                    int LC, int K, int nst, Consts<N> cs,
                                                    const double *__restrict__ bra,
                                                    const double *__restrict__ ket,
@@ -285,8 +285,8 @@ __global__ void __launch_bounds__(32, MINW) fsym_kernel(const int2 *__restrict__
     __shared__ double sacc[2 * Part<N>::size * 32];
     __shared__ double krow[2 * 16 * 33];
     __shared__ double kred[32];
-    const int t = blockIdx.x;
-    if (t >= ntiles) return;
+    const int t = t_begin + blockIdx.x;
+    if (t >= t_end) return;
     fsym_tile<N, VKET>(t, tiles[t], LC, K, nst, cs, bra, ket, C, kmap, H, S, part_b, part_k, status,
                        FusedSmem{sacc, krow, kred});
 }
@@ -298,11 +298,11 @@ __global__ void __launch_bounds__(256) fsym_sum_kernel(const int *__restrict__ t
                                                        const double *__restrict__ part_b,
                                                        const double *__restrict__ part_k,
                                                        const double *__restrict__ scal,
-                                                       double *__restrict__ out) {
+                                                       double *__restrict__ out, int t0, int t1) {
     const int id = blockIdx.x * blockDim.x + threadIdx.x;
     if (id >= Part<N>::size * K) return;
     const int f = id / K, m = id - f * K;
-    out[(size_t)f * K + m] = fsym_sum_one<N>(tstart, LC, K, f, m, part_b, part_k, scal[0]);
+    out[(size_t)f * K + m] = fsym_sum_one<N>(tstart, LC, K, f, m, part_b, part_k, scal[0], t0, t1);
 }
 
 // Sum the symmetric-pass partials of basis m into out[f * K + m]: its bra
@@ -636,8 +636,10 @@ template <int N> struct Launch {
     template <int MINW, bool VKET> static void fsym_v(const LaunchArgs &a, cudaStream_t st) {
         if constexpr (Part<N>::size <= 32) {
             Consts<N> cs = make_consts<N>(a.mass_h, a.ncv_h, a.efs);
-            fsym_kernel<N, MINW, VKET><<<a.nstiles, 32, 0, st>>>(
-                a.stiles, a.nstiles, a.LC_s, a.K, a.nst, cs, a.bra, a.ket, a.C, a.kmap, a.H, a.S, a.psym,
+            const int t0 = a.st_end > 0 ? a.st_begin : 0, t1 = a.st_end > 0 ? a.st_end : a.nstiles;
+            if (t1 <= t0) return;
+            fsym_kernel<N, MINW, VKET><<<t1 - t0, 32, 0, st>>>(
+                a.stiles, t0, t1, a.LC_s, a.K, a.nst, cs, a.bra, a.ket, a.C, a.kmap, a.H, a.S, a.psym,
                 a.psym + (size_t)a.nstiles * 2 * Part<N>::size * 32, a.status);
         }
     }
@@ -653,10 +655,13 @@ template <int N> struct Launch {
     static void fsym_reduce(const LaunchArgs &a, cudaStream_t st) {
         if constexpr (Part<N>::size <= 32) {
             constexpr int PS = Part<N>::size;
+            const int t0 = a.st_end > 0 ? a.st_begin : 0, t1 = a.st_end > 0 ? a.st_end : a.nstiles;
             fsym_sum_kernel<N><<<(PS * a.K + 255) / 256, 256, 0, st>>>(
-                a.stile_start, a.LC_s, a.K, a.psym, a.psym + (size_t)a.nstiles * 2 * PS * 32, a.scal, a.part);
-            grad_reduce_kernel<N><<<(a.K + 127) / 128, 128, 0, st>>>(a.part, a.K, a.bra, a.C, a.scal, a.g,
-                                                                      a.status);
+                a.stile_start, a.LC_s, a.K, a.psym, a.psym + (size_t)a.nstiles * 2 * PS * 32, a.scal,
+                a.sums ? a.sums : a.part, t0, t1);
+            if (!a.sums)
+                grad_reduce_kernel<N><<<(a.K + 127) / 128, 128, 0, st>>>(a.part, a.K, a.bra, a.C, a.scal, a.g,
+                                                                          a.status);
         }
     }
     static void rrms(const LaunchArgs &a, const int *terms, int nterms, double *out, cudaStream_t st) {
@@ -669,6 +674,9 @@ template <int N> struct Launch {
         dipole_kernel<N><<<a.ntiles, 32, 0, st>>>(a.tiles, a.ntiles, a.LC_e, a.K, a.nst, cs, a.ket, a.C, part,
                                                   a.status);
         dipole_sum_kernel<N><<<1, 256, 0, st>>>(part, a.ntiles, cs, comps, dip);
+    }
+    static void reduce_sums(const LaunchArgs &a, const double *sums, cudaStream_t st) {
+        grad_reduce_kernel<N><<<(a.K + 127) / 128, 128, 0, st>>>(sums, a.K, a.bra, a.C, a.scal, a.g, a.status);
     }
     static void matel(const LaunchArgs &a, const int *terms, int nterms, double *out,
                       cudaStream_t st) {
@@ -735,6 +743,10 @@ int launch_fsym_reduce(const LaunchArgs &a, cudaStream_t st) {
     NECG_DISPATCH(a.n, fsym_reduce(a, st));
     return 0;
 }
+int launch_reduce_sums(const LaunchArgs &a, const double *sums, cudaStream_t st) {
+    NECG_DISPATCH(a.n, reduce_sums(a, sums, st));
+    return 0;
+}
 int launch_rrms(const LaunchArgs &a, const int *terms, int nterms, double *out, cudaStream_t st) {
     NECG_DISPATCH(a.n, rrms(a, terms, nterms, out, st));
     return 0;
@@ -757,6 +769,13 @@ void launch_rows_finalize(const LaunchArgs &a, double *f_out, double *gradc, int
     rows_kernel<<<(a.K * 32 + 255) / 256, 256, 0, st>>>(a.H, a.S, a.C, a.K, a.rows);
     finalize_kernel<<<1, 1024, 0, st>>>(a.rows, a.C, a.K, a.scal, f_out, gradc, a.status, given, eng,
                                         norm, given_dev, en_out);
+}
+void launch_rows(const LaunchArgs &a, double *rows, cudaStream_t st) {
+    rows_kernel<<<(a.K * 32 + 255) / 256, 256, 0, st>>>(a.H, a.S, a.C, a.K, rows);
+}
+void launch_finalize(const LaunchArgs &a, const double *rows, double *f_out, double *gradc, cudaStream_t st) {
+    finalize_kernel<<<1, 1024, 0, st>>>(rows, a.C, a.K, a.scal, f_out, gradc, a.status, 0, 0.0, 0.0, nullptr,
+                                        nullptr);
 }
 void launch_reset_status(int *status, cudaStream_t st) { reset_status_kernel<<<1, 1, 0, st>>>(status); }
 void launch_fp64_probe(int blocks, int iters, double *sink, cudaStream_t st) {

@@ -27,6 +27,10 @@ struct LaunchArgs {
     const int *stile_start;                // first tile of each 32-row block (nkb + 1)
     int nstiles, LC_s, minb_s;
     double *psym;                          // bra partials, then ket partials
+    // shard of the fused pass: tiles [st_begin, st_end) (st_end = 0: all);
+    // sums (non-null): write the per-basis sums there and stop before GRADA
+    int st_begin, st_end;
+    double *sums;
 };
 
 int launch_prep(const LaunchArgs &a, cudaStream_t st);
@@ -53,6 +57,11 @@ void launch_rows_finalize(const LaunchArgs &a, double *f_out, double *gradc, int
                           double eng, double norm, cudaStream_t st,
                           const double *given_dev = nullptr, double *en_out = nullptr);
 void launch_reset_status(int *status, cudaStream_t st);
+// pieces of a sharded evaluation: rows (H C, S C) of this shard's H and S;
+// E, norm and GRADC from given rows; GRADA from given per-basis sums
+void launch_rows(const LaunchArgs &a, double *rows, cudaStream_t st);
+void launch_finalize(const LaunchArgs &a, const double *rows, double *f_out, double *gradc, cudaStream_t st);
+int launch_reduce_sums(const LaunchArgs &a, const double *sums, cudaStream_t st);
 void launch_fp64_probe(int blocks, int iters, double *sink, cudaStream_t st);
 void launch_f0(const double *z, int count, double *f, double *df, cudaStream_t st);
 

@@ -78,6 +78,17 @@ class Engine:
     def workspace_bytes(self) -> int:
         return int(self.L.necg_workspace_bytes(self.h))
 
+    def prepare_fused(self, K: int) -> int:
+        """Build the fused pass's tile list and partial buffers for bases of K
+        functions now (else the first batched step does it); returns the tile
+        count, or 0 when the symmetry set does not allow the fused pass."""
+        n = ctypes.c_int(0)
+        rc = self.L.necg_shard_tiles(self.h, int(K), ctypes.byref(n))
+        if rc == _lib.NECG_ERR_UNSUPPORTED:
+            return 0
+        _lib.check(rc, "necg_shard_tiles")
+        return n.value
+
     def set_tiles(self, lc_energy: int, lc_grad: int) -> None:
         _lib.check(self.L.necg_set_tiles(self.h, int(lc_energy), int(lc_grad)), "necg_set_tiles")
 

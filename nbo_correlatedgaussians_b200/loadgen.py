@@ -82,9 +82,14 @@ def served_stream(problems: list[Problem], maxfun: int, rate: float = 20.0, seed
     t_arr = arrival_times(len(problems), rate, seed)
     evals = [0] * len(problems)
     errors = []
+    # all runs at t = 0 and all admissible at once: time from the moment every
+    # run is admitted (setup excluded, as in plain_stream) -- the capacity
+    from .serve import workspace_estimate
+    saturate = rate <= 0 and len(problems) <= max_slots and \
+        sum(workspace_estimate(p) for p in problems) <= budget_bytes
+    gate = threading.Barrier(len(problems) + 1) if saturate else None
     with Server(budget_bytes=budget_bytes, max_slots=max_slots, tune=tune) as srv:
         t0 = time.perf_counter()
-        srv.t_start = t0
 
         def client(j):
             try:
@@ -92,14 +97,25 @@ def served_stream(problems: list[Problem], maxfun: int, rate: float = 20.0, seed
                 if dt > 0:
                     time.sleep(dt)
                 run = srv.open_run(problems[j])
+                if gate is not None:
+                    gate.wait()
                 evals[j] = tn_run(lambda x: srv.evaluate(run, x), problems[j].x.copy(), maxfun)
                 srv.close_run(run)
             except Exception as exc:  # noqa: BLE001 -- reported by the caller
                 errors.append((j, repr(exc)))
+                if gate is not None:
+                    gate.abort()
 
         th = [threading.Thread(target=client, args=(j,), daemon=True) for j in range(len(problems))]
         for t in th:
             t.start()
+        if gate is not None:
+            try:
+                gate.wait()
+            except threading.BrokenBarrierError:
+                pass
+            t0 = time.perf_counter()
+        srv.t_start = t0
         for t in th:
             t.join()
         wall = time.perf_counter() - t0
@@ -109,5 +125,6 @@ def served_stream(problems: list[Problem], maxfun: int, rate: float = 20.0, seed
     total = int(sum(evals))
     return {"runs": len(problems), "evals": total, "wall_s": wall, "evals_per_s": total / wall,
             "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "steps": st["steps"],
-            "mean_batch": st["mean_batch"], "arrival_rate_per_s": rate,
+            "mean_batch": st["mean_batch"], "gpu_step_s": st["gpu_step_s"], "plan_s": st["plan_s"],
+            "arrival_rate_per_s": rate,
             "last_arrival_s": float(t_arr[-1]) if len(t_arr) else 0.0}

@@ -86,8 +86,44 @@ def dipole() -> tuple[np.ndarray, np.ndarray]:
     return _state.engine().dipole(sh.iv, sh.C)
 
 
-def main(input_file: str = "oldquit.dat", maxiter: int = 20, output: str | None = None) -> dict:
-    """Run the driver; returns the quantities it prints (for tests and callers)."""
+class _IterationCap(Exception):
+    pass
+
+
+def optimise(fun, x0: np.ndarray, method: str = "L-BFGS-B", maxiter: int = 20, nvar: int | None = None):
+    """Minimise fun (returning (f, g)) from x0.  L-BFGS-B with the options of
+    python/necg.py:159-171; or "TNC" (SciPy's truncated Newton, the analogue of
+    the Fortran driver's LMQN, source/tn.f) stopped after ``maxiter``
+    iterations.  Returns (x, f, nit, message)."""
+    eps = 2.220446649250313e-16
+    nvar = nvar or x0.size
+    if method == "L-BFGS-B":
+        r = minimize(fun, x0, method="L-BFGS-B", jac=True,
+                     options={"maxiter": maxiter, "maxfun": 150 * nvar, "ftol": eps, "gtol": np.sqrt(eps)})
+        return r.x, float(r.fun), int(r.nit), str(r.message)
+    if method != "TNC":
+        raise ValueError(f"unknown method {method!r}")
+    last = {"x": x0.copy(), "it": 0}
+
+    def cb(xk):  # TNC has no iteration limit of its own
+        last["x"] = np.array(xk, dtype=np.float64)
+        last["it"] += 1
+        if last["it"] >= maxiter:
+            raise _IterationCap
+
+    try:
+        r = minimize(fun, x0, method="TNC", jac=True, callback=cb, options={"maxfun": 1000 * maxiter})
+        return r.x, float(r.fun), int(r.nit), str(r.message)
+    except _IterationCap:
+        f, _ = fun(last["x"])
+        return last["x"], float(f), last["it"], f"stopped after {maxiter} iterations"
+
+
+def main(input_file: str = "oldquit.dat", maxiter: int = 20, output: str | None = None,
+         method: str = "L-BFGS-B") -> dict:
+    """Run the driver; returns the quantities it prints (for tests and callers).
+    method "L-BFGS-B" is python/necg.py's optimiser; "TNC" runs ``maxiter``
+    truncated-Newton iterations instead."""
     if output is None:
         output = "necg.out"
     from . import utils
@@ -136,20 +172,16 @@ def main(input_file: str = "oldquit.dat", maxiter: int = 20, output: str | None 
         fvals.append(f)
         return f, g
 
-    eps = 2.220446649250313e-16
     t0 = time.perf_counter()
-    result = minimize(fun, hiv, method="L-BFGS-B", jac=True,
-                      options={"maxiter": maxiter, "maxfun": 150 * (sh.siv + sh.M), "ftol": eps,
-                               "gtol": np.sqrt(eps)})
+    x_opt, f_opt, nit, message = optimise(fun, hiv, method, maxiter, sh.siv + sh.M)
     res["t_optimise"] = time.perf_counter() - t0
     print(f"Time for energy/gradient calc. is {res['t_optimise']:.3f} seconds")
-    print(f"Energy is {result.fun:.15f} hartree")
-    print(f"Optimiser message: {result.message}")
-    res.update(f_opt=float(result.fun), x_opt=result.x.copy(), nit=int(result.nit), nfev=int(result.nfev),
-               fvals=np.array(fvals))
+    print(f"Energy is {f_opt:.15f} hartree")
+    print(f"Optimiser message: {message}")
+    res.update(f_opt=f_opt, x_opt=x_opt.copy(), nit=nit, nfev=len(fvals), fvals=np.array(fvals))
 
-    sh.iv[:] = result.x[:sh.siv]
-    sh.C[:] = result.x[sh.siv:]
+    sh.iv[:] = x_opt[:sh.siv]
+    sh.C[:] = x_opt[sh.siv:]
     print()
     print("***** The Output Vectors *****")
     print(sh.C)

@@ -93,6 +93,7 @@ class Server:
         self.waiting_runs: collections.deque[Run] = collections.deque()
         self.runs: dict[int, Run] = {}
         self.used = 0
+        self.pending_slots = 0  # admitted runs whose device state is being built
         self.next_id = 0
         self.latencies: list[float] = []
         self.steps = 0
@@ -103,6 +104,8 @@ class Server:
         self.stream = None
         self.t_start = None
         self.evals_done = 0
+        self.gpu_ms = 0.0   # device time of the batched steps (CUDA events on the server stream)
+        self.plan_s = 0.0   # host time spent planning steps
 
     # ----------------------------------------------------------- lifecycle
     def start(self) -> "Server":
@@ -139,7 +142,8 @@ class Server:
             if run.bytes > self.budget:
                 raise MemoryError(f"run needs {run.bytes} bytes, more than the whole budget {self.budget:.0f}")
             self.waiting_runs.append(run)
-            self._admit_locked()
+            ready = self._admit_locked()
+        self._materialise(ready)
         if not run.admitted.wait(timeout):
             raise TimeoutError("run was not admitted in time")
         return run
@@ -157,7 +161,8 @@ class Server:
                 run.engine = None
                 self.stream.synchronize()
                 eng.close()
-            self._admit_locked()
+            ready = self._admit_locked()
+        self._materialise(ready)
 
     def evaluate(self, run: Run, x: np.ndarray, timeout: float | None = None):
         """E and gradient at x = [iv, C] for this run (blocking)."""
@@ -173,15 +178,28 @@ class Server:
             raise req.error
         return req.f, req.g
 
-    def _admit_locked(self) -> None:
+    def _admit_locked(self) -> list[Run]:
+        """Reserve budget and a slot for every waiting run that fits (in arrival
+        order); the caller builds their device state outside the lock."""
+        ready = []
         while self.waiting_runs:
             run = self.waiting_runs[0]
-            if len(self.runs) >= self.max_slots or self.used + run.bytes > self.budget:
-                return
+            if len(self.runs) + self.pending_slots >= self.max_slots or self.used + run.bytes > self.budget:
+                break
             self.waiting_runs.popleft()
+            self.used += run.bytes
+            self.pending_slots += 1
+            ready.append(run)
+        return ready
+
+    def _materialise(self, runs: list[Run]) -> None:
+        """Device state of newly admitted runs: engine (handle + workspace,
+        tuned tiles, the fused pass's partial buffers) and resident x, g, f.
+        Runs outside the server lock, so steps keep being planned meanwhile."""
+        for run in runs:
             p = run.problem
             with torch.cuda.device(self.device):
-                run.engine = Engine(p, device=self.device)
+                eng = Engine(p, device=self.device)
                 run.x = torch.from_numpy(np.ascontiguousarray(p.x)).to(self.device)
                 run.g = torch.empty_like(run.x)
                 run.f = torch.zeros(1, dtype=torch.float64, device=self.device)
@@ -189,9 +207,12 @@ class Server:
                 run.gh = torch.empty(run.x.numel(), dtype=torch.float64).pin_memory()
                 run.fh = torch.empty(1, dtype=torch.float64).pin_memory()
                 if self.tune:
-                    tuned(run.engine, run.x, p.K)
-            self.used += run.bytes
-            self.runs[run.id] = run
+                    tuned(eng, run.x, p.K)
+                eng.prepare_fused(p.K)
+            with self.lock:
+                run.engine = eng
+                self.pending_slots -= 1
+                self.runs[run.id] = run
             run.admitted.set()
 
     # -------------------------------------------------------------- worker
@@ -230,9 +251,15 @@ class Server:
                 r.run.xh.numpy()[:] = r.x
                 r.run.x.copy_(r.run.xh, non_blocking=True)
             runs = [r.run for r in reqs]
+            t0 = time.perf_counter()
             batch.plan([u.engine for u in runs], [u.problem.K for u in runs], [u.x for u in runs],
                        [u.g for u in runs], [u.f for u in runs], stream=s)
+            self.plan_s += time.perf_counter() - t0
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(s)
             batch.step(self.graph, stream=s)
+            e1.record(s)
             for u in runs:
                 u.gh.copy_(u.g, non_blocking=True)
                 u.fh.copy_(u.f, non_blocking=True)
@@ -240,10 +267,11 @@ class Server:
             ev.record(s)
         self.steps += 1
         self.step_sizes.append(len(reqs))
-        return reqs, ev, batch
+        return reqs, ev, batch, (e0, e1)
 
-    def _deliver(self, reqs: list[Request], ev, batch: Batch) -> None:
+    def _deliver(self, reqs: list[Request], ev, batch: Batch, timing) -> None:
         ev.synchronize()
+        self.gpu_ms += timing[0].elapsed_time(timing[1])
         codes = batch.status(stream=self.stream)
         now = time.perf_counter()
         for r, code in zip(reqs, codes):
@@ -268,4 +296,4 @@ class Server:
                 "mean_batch": float(np.mean(self.step_sizes)) if self.step_sizes else 0.0,
                 "p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
                 "evals_per_s": self.evals_done / wall if wall > 0 else 0.0, "wall_s": wall,
-                "hbm_used_bytes": self.used}
+                "gpu_step_s": self.gpu_ms * 1e-3, "plan_s": self.plan_s, "hbm_used_bytes": self.used}

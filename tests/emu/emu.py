@@ -135,3 +135,78 @@ def elements(p, terms):
             ctypes.c_int(len(t)), ctypes.c_void_p(_p(t)), ctypes.c_void_p(_p(mat)), ctypes.c_void_p(_p(tg)),
             ctypes.c_void_p(_p(tgs)))
     return rc, mat, tg, tgs
+
+
+class EmuShardOps:
+    """The shard steps of ``nbo_correlatedgaussians_b200.shard.DeviceShardOps``
+    run by the host emulation of the kernels, on CPU tensors, so that the
+    sharded orchestration (tile ranges, the two all-reduces, E and GRADC from
+    the summed rows) can be tested on CPU ranks with the gloo backend."""
+
+    def __init__(self, p, lc_s=2):
+        import torch
+        self.torch = torch
+        self.p = p
+        self.lc = int(lc_s)
+        self.n, self.blk = p.n, p.blk
+        self.ps = p.n * (p.n + 1) // 2 + 1 + 3 * p.n
+        self.device = torch.device("cpu")
+        self._sumH = self._sumS = None
+        self._status = 0
+
+    def _call_pairs(self, x, K, t0, t1):
+        L = lib()
+        c = _consts(self.p)
+        rows = np.zeros(2 * K)
+        sH = np.zeros(self.ps * K)
+        sS = np.zeros(self.ps * K)
+        nt = ctypes.c_int(0)
+        fn = L.emu_shard_pairs
+        fn.restype = ctypes.c_int
+        rc = fn(ctypes.c_int(self.p.n), ctypes.c_int(self.p.nst), ctypes.c_int(K), ctypes.c_double(self.p.efs),
+                *[ctypes.c_void_p(_p(a)) for a in c], ctypes.c_void_p(_p(x)), ctypes.c_int(self.lc),
+                ctypes.c_int(t0), ctypes.c_int(t1), ctypes.c_void_p(_p(rows)), ctypes.c_void_p(_p(sH)),
+                ctypes.c_void_p(_p(sS)), ctypes.byref(nt))
+        return rc, rows, sH, sS, nt.value
+
+    def tiles(self, K):
+        x = np.ascontiguousarray(self.p.x)
+        rc, _, _, _, nt = self._call_pairs(x, K, 0, 0)
+        assert rc >= 0
+        return nt
+
+    def pairs(self, x, K, t0, t1):
+        xn = np.ascontiguousarray(x.numpy())
+        rc, rows, self._sumH, self._sumS, _ = self._call_pairs(xn, K, t0, t1)
+        assert rc >= 0
+        self._status = 2 if rc & 1 else (3 if rc & 2 else 0)
+        return self.torch.from_numpy(rows)
+
+    def grad(self, x, K, rows, t0, t1):
+        # the finalize kernel: E, norm and GRADC from the summed rows
+        xn = x.numpy()
+        C = xn[K * self.blk:]
+        r = rows.numpy()
+        cHc, cSc = float(C @ r[:K]), float(C @ r[K:])
+        E, norm = cHc / cSc, 1.0 / cSc
+        g = np.zeros(K * self.blk + K)
+        g[K * self.blk:] = 2.0 * norm * (r[:K] - E * r[K:])
+        self._norm = norm
+        sums = self._sumH - E * self._sumS
+        return (self.torch.tensor([E], dtype=self.torch.float64), self.torch.from_numpy(g),
+                self.torch.from_numpy(sums))
+
+    def finish(self, x, K, sums, g):
+        L = lib()
+        c = _consts(self.p)
+        gn = np.ascontiguousarray(g.numpy()).copy()
+        fn = L.emu_shard_finish
+        fn.restype = ctypes.c_int
+        fn(ctypes.c_int(self.p.n), ctypes.c_int(self.p.nst), ctypes.c_int(K), ctypes.c_double(self.p.efs),
+           *[ctypes.c_void_p(_p(a)) for a in c], ctypes.c_void_p(_p(np.ascontiguousarray(x.numpy()))),
+           ctypes.c_void_p(_p(np.ascontiguousarray(sums.numpy()))), ctypes.c_double(self._norm),
+           ctypes.c_void_p(_p(gn)))
+        return self.torch.from_numpy(gn)
+
+    def status(self):
+        return self._status

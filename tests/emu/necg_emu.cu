@@ -502,6 +502,152 @@ template <int N> int dipole(const Args &a, const double *iv, const double *C, in
     return flags;
 }
 
+// Host mirror of one rank's share of a sharded evaluation (necg_shard_pairs and
+// the per-basis sums of necg_shard_grad): the fused tiles [t0, t1) only, with
+// H and S zero outside them; returns this shard's rows (H C, S C) and its
+// per-basis sums of the H and of the S gradient partials, kept apart (the
+// caller combines them once E is known from the summed rows).
+template <int N> int shard_pairs(const Args &a, const double *x, int LCs, int t0, int t1, double *rows,
+                                 double *sumH, double *sumS, int *ntiles_out) {
+    const int K = a.K, nst = a.nst;
+    constexpr int PS = Part<N>::size;
+    if (PS > 32) return -2;
+    const size_t siv = (size_t)K * (tri(N) + 3 * N);
+    const double *iv = x, *C = x + siv;
+    HostMap hm = build_map<N>(a);
+    if (!hm.ok) return -3;
+    Consts<N> cs = consts<N>(a.mass, a.ncv, a.efs);
+    std::vector<double> bra((size_t)BraLayout<N>::size * K), ket((size_t)KetLayout<N>::size * K * nst);
+    for (int k = 0; k < K; ++k) prep_bra_one<N>(iv, K, cs, bra.data(), k);
+    for (int id = 0; id < K * nst; ++id)
+        prep_ket_one<N>(iv, C, nst, cs, a.sml, a.sms, a.scvv, ket.data(), id, hm.pinv.data());
+    std::vector<int> tstart;
+    std::vector<std::pair<int, int>> tiles;
+    for (int kb = 0; kb * 32 < K; ++kb) {
+        tstart.push_back((int)tiles.size());
+        const int last = kb * 32 + 31 < K - 1 ? kb * 32 + 31 : K - 1;
+        for (int lc = 0; lc <= last / LCs; ++lc) tiles.push_back({kb, lc});
+    }
+    tstart.push_back((int)tiles.size());
+    const int nt = (int)tiles.size();
+    *ntiles_out = nt;
+    if (t0 < 0 || t1 > nt || t1 < t0) return -4;
+    std::vector<double> H((size_t)K * K, 0.0), S((size_t)K * K, 0.0);
+    std::vector<double> pb((size_t)nt * 2 * PS * 32, 0.0), pk((size_t)nt * LCs * 2 * PS, 0.0);
+    KetMap km{hm.cnt.data(), hm.src.data(), hm.coef.data(), hm.maxnz};
+    int flags = 0;
+    for (int t = t0; t < t1; ++t) {
+        const int kb = tiles[t].first, l0 = tiles[t].second * LCs, l1 = std::min(l0 + LCs, K);
+        std::vector<RegAcc<N, CD>> accH(32), accS(32);
+        for (int lane = 0; lane < 32; ++lane) {
+            accH[lane].zero();
+            accS[lane].zero();
+        }
+        for (int l = l0; l < l1; ++l) {
+            double aH[32] = {0.0}, aS[32] = {0.0};
+            double hsum[32] = {0.0}, ssum[32] = {0.0};
+            for (int P = 0; P < nst; ++P) {
+                const double *krp = ket.data() + ((size_t)l * nst + P) * KetLayout<N>::size;
+                double rowsH[32][33], rowsS[32][33];
+                for (int lane = 0; lane < 32; ++lane) {
+                    const int k = kb * 32 + lane;
+                    for (int ff = 0; ff < PS; ++ff) rowsH[lane][ff] = rowsS[lane][ff] = 0.0;
+                    if (k < K && l <= k) {
+                        const double wk = l < k ? 2.0 * C[k] * krp[KetLayout<N>::winv] : 0.0;
+                        RowOutH roH{rowsH[lane]}, roS{rowsS[lane]};
+                        CD h, ov;
+                        if (!term_fused<N, CD>(HostBra{bra.data() + k, (size_t)K}, HostKet{krp}, cs,
+                                               CD(krp[KetLayout<N>::wC]), CD(wk), accH[lane], accS[lane], roH,
+                                               roS, h, ov))
+                            flags |= 1;
+                        hsum[lane] += krp[KetLayout<N>::w] * h.v;
+                        ssum[lane] += krp[KetLayout<N>::w] * ov.v;
+                    }
+                }
+                for (int which = 0; which < 2; ++which) {
+                    double red[32];
+                    for (int j = 0; j < 32; ++j) {
+                        double v = 0.0;
+                        if (j < PS)
+                            for (int r = 0; r < 16; ++r)
+                                v += which ? rowsS[2 * r][j] + rowsS[2 * r + 1][j]
+                                           : rowsH[2 * r][j] + rowsH[2 * r + 1][j];
+                        red[j] = v;
+                    }
+                    for (int j = 0; j < PS; ++j) (which ? aS : aH)[j] += ket_map_apply(km, P, j, PS, red);
+                }
+            }
+            for (int lane = 0; lane < 32; ++lane) {
+                const int k = kb * 32 + lane;
+                if (k < K && l <= k) {
+                    H[(size_t)k * K + l] = H[(size_t)l * K + k] = hsum[lane];
+                    S[(size_t)k * K + l] = S[(size_t)l * K + k] = ssum[lane];
+                }
+            }
+            for (int j = 0; j < PS; ++j) {
+                pk[(((size_t)t * LCs + (l - l0)) * 2 + 0) * PS + j] = aH[j];
+                pk[(((size_t)t * LCs + (l - l0)) * 2 + 1) * PS + j] = aS[j];
+            }
+        }
+        for (int lane = 0; lane < 32; ++lane) {
+            if (kb * 32 + lane >= K) continue;
+            for (int which = 0; which < 2; ++which) {
+                RegAcc<N, CD> &ac = which ? accS[lane] : accH[lane];
+                const size_t base = ((size_t)t * 2 + which) * PS;
+                for (int tt = 0; tt < tri(N); ++tt) pb[(base + tt) * 32 + lane] = ac.g(tt).v;
+                pb[(base + tri(N)) * 32 + lane] = ac.d().v;
+                for (int tt = 0; tt < 3 * N; ++tt) pb[(base + tri(N) + 1 + tt) * 32 + lane] = ac.s(tt).v;
+            }
+        }
+    }
+    for (int i = 0; i < K; ++i) {
+        double hh = 0.0, ss = 0.0;
+        for (int j = 0; j < K; ++j) {
+            hh += H[(size_t)i * K + j] * C[j];
+            ss += S[(size_t)i * K + j] * C[j];
+        }
+        rows[i] = hh;
+        rows[K + i] = ss;
+    }
+    const int nkb = (K + 31) / 32;
+    for (int ff = 0; ff < PS; ++ff)
+        for (int m = 0; m < K; ++m) {
+            const int kb = m / 32, lane = m % 32;
+            double sH = 0.0, sS = 0.0;
+            for (int t = std::max(tstart[kb], t0); t < std::min(tstart[kb + 1], t1); ++t) {
+                sH += pb[(((size_t)t * 2 + 0) * PS + ff) * 32 + lane];
+                sS += pb[(((size_t)t * 2 + 1) * PS + ff) * 32 + lane];
+            }
+            const int lc = m / LCs, ll = m % LCs;
+            int kb0 = lc * LCs - 31;
+            kb0 = kb0 > 0 ? (kb0 + 31) / 32 : 0;
+            for (int q = kb0; q < nkb; ++q) {
+                const int t = tstart[q] + lc;
+                if (t < t0 || t >= t1) continue;
+                const size_t base = ((size_t)t * LCs + ll) * 2;
+                sH += pk[(base + 0) * PS + ff];
+                sS += pk[(base + 1) * PS + ff];
+            }
+            sumH[(size_t)ff * K + m] = sH;
+            sumS[(size_t)ff * K + m] = sS;
+        }
+    return flags;
+}
+
+// GRADA from summed per-basis sums (necg_shard_finish): g[block k] from
+// sums[f * K + k] scaled by norm C_k.
+template <int N> int shard_finish(const Args &a, const double *x, const double *sums, double norm, double *g) {
+    const int K = a.K;
+    const size_t siv = (size_t)K * (tri(N) + 3 * N);
+    Consts<N> cs = consts<N>(a.mass, a.ncv, a.efs);
+    std::vector<double> bra((size_t)BraLayout<N>::size * K);
+    for (int k = 0; k < K; ++k) prep_bra_one<N>(x, K, cs, bra.data(), k);
+    int flags = 0;
+    for (int k = 0; k < K; ++k)
+        if (!grad_reduce_one<N>(sums, 1, K, bra.data(), norm * x[siv + k], g, k)) flags |= 2;
+    return flags;
+}
+
 template <int N>
 int elements(const Args &a, const double *iv, int nterms, const int *terms, double *mat,
              double *tg, double *tgs) {
@@ -569,6 +715,21 @@ extern "C" int emu_dipole(int n, int nst, int K, double efs, const double *mass,
                           const double *C, int lc, double *comps, double *dip) {
     Args a{nst, K, efs, mass, ncv, scvv, sml, sms};
     EMU_DISPATCH(n, (dipole<N>(a, iv, C, lc, comps, dip)));
+}
+
+extern "C" int emu_shard_pairs(int n, int nst, int K, double efs, const double *mass, const double *ncv,
+                               const double *scvv, const double *sml, const double *sms, const double *x,
+                               int lc_s, int t0, int t1, double *rows, double *sumH, double *sumS,
+                               int *ntiles) {
+    Args a{nst, K, efs, mass, ncv, scvv, sml, sms};
+    EMU_DISPATCH(n, (shard_pairs<N>(a, x, lc_s, t0, t1, rows, sumH, sumS, ntiles)));
+}
+
+extern "C" int emu_shard_finish(int n, int nst, int K, double efs, const double *mass, const double *ncv,
+                                const double *scvv, const double *sml, const double *sms, const double *x,
+                                const double *sums, double norm, double *g) {
+    Args a{nst, K, efs, mass, ncv, scvv, sml, sms};
+    EMU_DISPATCH(n, (shard_finish<N>(a, x, sums, norm, g)));
 }
 
 extern "C" int emu_elements(int n, int nst, int K, double efs, const double *mass, const double *ncv,

@@ -22,6 +22,9 @@ Fixtures (npz, all FP64):
                   energetics, the L-BFGS-B result (20 iterations, main's
                   options), the energetics at the optimum and the dipole
                   components.
+  driver_tnc_oldquit.npz  the same start point optimised with SciPy's TNC
+                  (truncated Newton) for at most 50 iterations through the
+                  reference's outprod: iterate count, final E and x.
 Select generators by name on the command line (default: all).
 The reference is imported only by this script; the tests read the npz files.
 """
@@ -255,8 +258,36 @@ def gen_driver(maxiter: int = 20):
     print("driver: eig0", ev[0], "en0", en0, "f_opt", res.fun, "nit", res.nit, "en1", en1, "dipole", dip)
 
 
+class _Cap(Exception):
+    pass
+
+
+def gen_driver_tnc(maxiter: int = 50):
+    from scipy.optimize import minimize
+    d = np.load(os.path.join(HERE, "driver_oldquit.npz"))
+    read_input(os.path.join(REF, "oldquit.dat"))
+    x0 = np.concatenate([sh.iv.copy(), d["C0"]])
+    last = {"x": x0.copy(), "it": 0}
+
+    def cb(xk):
+        last["x"] = np.array(xk)
+        last["it"] += 1
+        if last["it"] >= maxiter:
+            raise _Cap
+
+    try:
+        r = minimize(outprod, x0, method="TNC", jac=True, callback=cb, options={"maxfun": 1000 * maxiter})
+        x, f, nit = r.x, float(r.fun), int(r.nit)
+    except _Cap:
+        x, nit = last["x"], last["it"]
+        f = float(outprod(x)[0])
+    np.savez(os.path.join(HERE, "driver_tnc_oldquit.npz"), x_opt=x, f_opt=f, nit=nit, maxiter=maxiter)
+    print("driver TNC: f", f, "nit", nit)
+
+
 if __name__ == "__main__":
-    want = set(sys.argv[1:]) or {"f0", "f0_edge", "oldquit", "elements", "outprod", "rrms", "driver"}
+    want = set(sys.argv[1:]) or {"f0", "f0_edge", "oldquit", "elements", "outprod", "rrms", "driver",
+                                 "driver_tnc"}
     if "f0" in want:
         gen_f0()
     if "f0_edge" in want:
@@ -275,3 +306,5 @@ if __name__ == "__main__":
             gen_rrms(system)
     if "driver" in want:
         gen_driver()
+    if "driver_tnc" in want:
+        gen_driver_tnc()

@@ -44,16 +44,18 @@ def test_autograd_backward_is_the_gradient_kernel(torch_cuda):
 
 
 def test_autograd_central_differences(torch_cuda):
-    """Config 2 check at a reduced size: the autograd gradient against the
-    oracle's gradel-based gradient (1e-9 norm-wise) and against finite
-    differences on 64 random parameters: central h = 1e-6 (the requested check;
+    """H2 K=2048 (n=3, nst=4, seed 2): E through the autograd Function, its
+    gradient (the hand-written backward) against the oracle's gradel-based
+    gradient (1e-9 norm-wise) and against finite differences on 64 random
+    parameters (indices from seed 2): central h = 1e-6 (the requested check;
     round-off in E limits it to ~1e-6 relative, so it is bounded at 1e-5) and a
-    5-point stencil with h = 1e-4 (bounded at 1e-7)."""
+    5-point stencil with h = 1e-4 (bounded at 1e-7).  C is random (seed 7): with
+    C = 1/K the gradient components are small and the FD quotients noisier."""
     torch = torch_cuda
     from nbo_correlatedgaussians_b200 import synth
     from nbo_correlatedgaussians_b200.autograd import energy
     from nbo_correlatedgaussians_b200.engine import Engine
-    p = synth.make_problem("H2", 128, 2)
+    p = synth.workload("h2_k2048")
     p.C = np.random.default_rng(7).normal(size=p.K)
     eng = Engine(p)
     x = torch.tensor(p.x, device="cuda")
@@ -62,7 +64,8 @@ def test_autograd_central_differences(torch_cuda):
     E = energy(xg[:siv], xg[siv:], eng)
     E.backward()
     g = xg.grad.cpu().numpy()
-    _, go = Oracle.from_problem(p).outprod(p.x, nthreads=8)
+    import os
+    _, go = Oracle.from_problem(p).outprod(p.x, nthreads=len(os.sched_getaffinity(0)))
     assert normwise(g, go) < TOL_G
     idx = np.random.default_rng(2).choice(p.x.size, 64, replace=False)
 
