@@ -437,12 +437,12 @@ int necg_outprod(necg_handle *h, int K, const double *x_dev, double *f_dev, doub
         mark(h, 0, st);
         if (necg::launch_prep(a, st)) return NECG_ERR_UNSUPPORTED;
         mark(h, 1, st);
-        necg::launch_fsym(a, st);
+        if (necg::launch_fsym(a, st)) return NECG_ERR_ARG;
         mark(h, 2, st);
         necg::launch_rows_finalize(a, f_dev, g_dev + siv, 0, 0.0, 0.0, st);
         mark(h, 3, st);
         mark(h, 4, st);
-        necg::launch_fsym_reduce(a, st);
+        if (necg::launch_fsym_reduce(a, st)) return NECG_ERR_ARG;
         mark(h, 5, st);
         return finish_launch();
     }
@@ -470,6 +470,8 @@ int shard_args(necg_handle *h, int K, const double *x_dev, int t0, int t1, cudaS
     const size_t siv = (size_t)K * (h->n * (h->n + 1) / 2 + 3 * h->n);
     a.iv = x_dev;
     a.C = x_dev + siv;
+    a.H = h->d_H;
+    a.S = h->d_S;
     a.stiles = h->d_stiles;
     a.stile_start = h->d_stile_start;
     a.nstiles = h->nstiles;
@@ -504,8 +506,8 @@ int necg_shard_pairs(necg_handle *h, int K, const double *x_dev, int tile_begin,
     CK(cudaMemsetAsync(h->d_H, 0, sizeof(double) * (size_t)K * K, st));
     CK(cudaMemsetAsync(h->d_S, 0, sizeof(double) * (size_t)K * K, st));
     if (necg::launch_prep(a, st)) return NECG_ERR_UNSUPPORTED;
-    if (tile_end > tile_begin) necg::launch_fsym(a, st);
-    necg::launch_rows(a, rows_dev, st);
+    if (tile_end > tile_begin && necg::launch_fsym(a, st)) return NECG_ERR_ARG;
+    if (necg::launch_rows(a, rows_dev, st)) return NECG_ERR_ARG;
     return finish_launch();
 }
 
@@ -521,7 +523,7 @@ int necg_shard_grad(necg_handle *h, int K, const double *x_dev, const double *ro
     a.g = g_dev;
     a.sums = sums_dev;
     necg::launch_finalize(a, rows_dev, f_dev, g_dev + siv, st);
-    necg::launch_fsym_reduce(a, st);  // per-basis sums of this shard's tiles only
+    if (necg::launch_fsym_reduce(a, st)) return NECG_ERR_ARG;  // per-basis sums of this shard's tiles only
     return finish_launch();
 }
 
@@ -538,7 +540,7 @@ int necg_shard_finish(necg_handle *h, int K, const double *x_dev, const double *
     a.iv = x_dev;
     a.C = x_dev + siv;
     a.g = g_dev;
-    necg::launch_reduce_sums(a, sums_dev, st);
+    if (necg::launch_reduce_sums(a, sums_dev, st)) return NECG_ERR_ARG;
     return finish_launch();
 }
 

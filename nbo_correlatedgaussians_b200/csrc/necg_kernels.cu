@@ -291,18 +291,53 @@ __global__ void __launch_bounds__(32, MINW) fsym_kernel(const int2 *__restrict__
                        FusedSmem{sacc, krow, kred});
 }
 
-// Sum the fused-pass partials of basis m and combine out[f * K + m] =
-// sum_H - E sum_S with E = scal[0], written by finalize after the pass.
+// Sum the fused-pass partials and combine out[f * K + m] = sum_H - E sum_S with
+// E = scal[0] (written by finalize after the pass).  Block (kb, f): the 32
+// bases of row block kb, field f.  Their bra partials come from every tile of
+// block kb (up to K / LC of them), so the 8 warps of the block take every 8th
+// tile and their sums are combined in a fixed order; the ket partials (one
+// tile per later row block) are added by the first warp.  Only tiles in
+// [t0, t1) count (a shard of the pass).
 template <int N>
 __global__ void __launch_bounds__(256) fsym_sum_kernel(const int *__restrict__ tstart, int LC, int K,
                                                        const double *__restrict__ part_b,
                                                        const double *__restrict__ part_k,
                                                        const double *__restrict__ scal,
                                                        double *__restrict__ out, int t0, int t1) {
-    const int id = blockIdx.x * blockDim.x + threadIdx.x;
-    if (id >= Part<N>::size * K) return;
-    const int f = id / K, m = id - f * K;
-    out[(size_t)f * K + m] = fsym_sum_one<N>(tstart, LC, K, f, m, part_b, part_k, scal[0], t0, t1);
+    constexpr int PS = Part<N>::size;
+    __shared__ double red[2][8][32];
+    const int kb = blockIdx.x, f = blockIdx.y;
+    const int lane = threadIdx.x & 31, seg = threadIdx.x >> 5;
+    const int m = kb * 32 + lane;
+    const int ta = max(tstart[kb], t0), tb = min(tstart[kb + 1], t1);
+    double sH = 0.0, sS = 0.0;
+    for (int t = ta + seg; t < tb; t += 8) {
+        sH += part_b[(((size_t)t * 2 + 0) * PS + f) * 32 + lane];
+        sS += part_b[(((size_t)t * 2 + 1) * PS + f) * 32 + lane];
+    }
+    red[0][seg][lane] = sH;
+    red[1][seg][lane] = sS;
+    __syncthreads();
+    if (seg != 0 || m >= K) return;
+    sH = red[0][0][lane];
+    sS = red[1][0][lane];
+#pragma unroll
+    for (int q = 1; q < 8; ++q) {
+        sH += red[0][q][lane];
+        sS += red[1][q][lane];
+    }
+    const int lc = m / LC, ll = m - lc * LC;
+    const int nkb = (K + 31) >> 5;
+    int kb0 = lc * LC - 31;
+    kb0 = kb0 > 0 ? (kb0 + 31) >> 5 : 0;
+    for (int q = kb0; q < nkb; ++q) {
+        const int t = tstart[q] + lc;
+        if (t < t0 || t >= t1) continue;
+        const size_t base = ((size_t)t * LC + ll) * 2;
+        sH += part_k[(base + 0) * PS + f];
+        sS += part_k[(base + 1) * PS + f];
+    }
+    out[(size_t)f * K + m] = sH - scal[0] * sS;
 }
 
 // Sum the symmetric-pass partials of basis m into out[f * K + m]: its bra
@@ -656,7 +691,7 @@ template <int N> struct Launch {
         if constexpr (Part<N>::size <= 32) {
             constexpr int PS = Part<N>::size;
             const int t0 = a.st_end > 0 ? a.st_begin : 0, t1 = a.st_end > 0 ? a.st_end : a.nstiles;
-            fsym_sum_kernel<N><<<(PS * a.K + 255) / 256, 256, 0, st>>>(
+            fsym_sum_kernel<N><<<dim3((a.K + 31) / 32, PS), 256, 0, st>>>(
                 a.stile_start, a.LC_s, a.K, a.psym, a.psym + (size_t)a.nstiles * 2 * PS * 32, a.scal,
                 a.sums ? a.sums : a.part, t0, t1);
             if (!a.sums)
@@ -735,15 +770,19 @@ int launch_gsym_reduce(const LaunchArgs &a, cudaStream_t st) {
 }
 int launch_fsym(const LaunchArgs &a, cudaStream_t st) {
     if (a.n > 5) return -1;
+    // every buffer the pass writes must be set (no launch on a null pointer)
+    if (!a.H || !a.S || !a.psym || !a.stiles || !a.bra || !a.ket || !a.C || !a.status) return -1;
     NECG_DISPATCH(a.n, fsym_tiles(a, st));
     return 0;
 }
 int launch_fsym_reduce(const LaunchArgs &a, cudaStream_t st) {
     if (a.n > 5) return -1;
+    if (!a.stile_start || !a.psym || !a.scal || (!a.sums && (!a.part || !a.bra || !a.C || !a.g))) return -1;
     NECG_DISPATCH(a.n, fsym_reduce(a, st));
     return 0;
 }
 int launch_reduce_sums(const LaunchArgs &a, const double *sums, cudaStream_t st) {
+    if (!sums || !a.bra || !a.C || !a.scal || !a.g || !a.status) return -1;
     NECG_DISPATCH(a.n, reduce_sums(a, sums, st));
     return 0;
 }
@@ -770,8 +809,10 @@ void launch_rows_finalize(const LaunchArgs &a, double *f_out, double *gradc, int
     finalize_kernel<<<1, 1024, 0, st>>>(a.rows, a.C, a.K, a.scal, f_out, gradc, a.status, given, eng,
                                         norm, given_dev, en_out);
 }
-void launch_rows(const LaunchArgs &a, double *rows, cudaStream_t st) {
+int launch_rows(const LaunchArgs &a, double *rows, cudaStream_t st) {
+    if (!a.H || !a.S || !a.C || !rows) return -1;
     rows_kernel<<<(a.K * 32 + 255) / 256, 256, 0, st>>>(a.H, a.S, a.C, a.K, rows);
+    return 0;
 }
 void launch_finalize(const LaunchArgs &a, const double *rows, double *f_out, double *gradc, cudaStream_t st) {
     finalize_kernel<<<1, 1024, 0, st>>>(rows, a.C, a.K, a.scal, f_out, gradc, a.status, 0, 0.0, 0.0, nullptr,

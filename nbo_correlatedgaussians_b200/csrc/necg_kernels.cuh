@@ -59,7 +59,7 @@ void launch_rows_finalize(const LaunchArgs &a, double *f_out, double *gradc, int
 void launch_reset_status(int *status, cudaStream_t st);
 // pieces of a sharded evaluation: rows (H C, S C) of this shard's H and S;
 // E, norm and GRADC from given rows; GRADA from given per-basis sums
-void launch_rows(const LaunchArgs &a, double *rows, cudaStream_t st);
+int launch_rows(const LaunchArgs &a, double *rows, cudaStream_t st);
 void launch_finalize(const LaunchArgs &a, const double *rows, double *f_out, double *gradc, cudaStream_t st);
 int launch_reduce_sums(const LaunchArgs &a, const double *sums, cudaStream_t st);
 void launch_fp64_probe(int blocks, int iters, double *sink, cudaStream_t st);

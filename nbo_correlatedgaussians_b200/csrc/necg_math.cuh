@@ -231,29 +231,33 @@ NECG_HD void symv3(const Acc &S, int off, const R (&x)[3 * N], R (&y)[3 * N]) {
 // Boys-function pieces for one Coulomb pair.  Given a = v^T Bi v and
 // bb = |v^T T|^2 (z = bb / a) returns fs = F0(z) a^{-1/2} and, when GRAD,
 // dfs = F0'(z) a^{-1/2} and ia = 1/a.  The Pade branch (z <= 16.3578) and the
-// asymptotic branch sqrt(pi/(4z)) follow python/utils.py:78-106.
+// asymptotic branch sqrt(pi/(4z)) follow python/utils.py:78-106; in the Pade
+// branch F0 = sqrt(num / den).  Two reciprocal square roots give every
+// quotient and root needed:
+//   ra = a^{-1/2}:          1/a = ra^2,  fs = F0 ra
+//   q = (num den)^{-1/2}:   F0 = num q,  1/num = q^2 den
+// and F0' a^{-1/2} = (num' - F0^2 den') fs / (2 num)  (from F0^2 = num / den).
 #pragma nv_exec_check_disable
 template <bool GRAD, typename R>
 NECG_HD void boys(R a, R bb, R &fs, R &dfs, R &ia, R &z) {
-    ia = R(1.0) / a;
+    const R ra = rsqrt(a);
+    ia = ra * ra;
     z = bb * ia;
     if (z <= NECG_F0_SPLIT) {
         const R num = ((((NECG_PC1 * z + NECG_PC2) * z + NECG_PC3) * z + NECG_PC4) * z +
                        NECG_PC5) * z + 1.0;
         const R den = (((((NECG_PC6 * z + NECG_PC7) * z + NECG_PC8) * z + NECG_PC9) * z +
                         NECG_PC10) * z + NECG_PC11) * z + 1.0;
+        const R q = rsqrt(num * den);
+        const R F0 = num * q;
+        fs = F0 * ra;
         if (GRAD) {
-            const R nd = R(1.0) / (num * den);
-            const R r = num * num * nd;  // num / den
-            fs = sqrt(r * ia);
             const R dN = (((5.0 * NECG_PC1 * z + 4.0 * NECG_PC2) * z + 3.0 * NECG_PC3) * z +
                           2.0 * NECG_PC4) * z + NECG_PC5;
             const R dD = ((((6.0 * NECG_PC6 * z + 5.0 * NECG_PC7) * z + 4.0 * NECG_PC8) * z +
                            3.0 * NECG_PC9) * z + 2.0 * NECG_PC10) * z + NECG_PC11;
-            // F0' = (dN - r dD) / (2 den F0);  F0' a^-1/2 = (dN - r dD) fs / (2 num)
-            dfs = 0.5 * (dN - r * dD) * fs * (den * nd);
+            dfs = 0.5 * (dN - F0 * F0 * dD) * fs * (q * q * den);
         } else {
-            fs = sqrt(num * ia / den);
             dfs = R(0.0);
         }
     } else {

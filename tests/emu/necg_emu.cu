@@ -396,10 +396,17 @@ template <int N> int outprod_fused(const Args &a, const double *x, int LCs, doub
     for (int ff = 0; ff < PS; ++ff)
         for (int m = 0; m < K; ++m) {
             const int kb = m / 32, lane = m % 32;
-            double sH = 0.0, sS = 0.0;
-            for (int t = tstart[kb]; t < tstart[kb + 1]; ++t) {
-                sH += pb[(((size_t)t * 2 + 0) * PS + ff) * 32 + lane];
-                sS += pb[(((size_t)t * 2 + 1) * PS + ff) * 32 + lane];
+            // the kernel's order: 8 segments (every 8th tile), combined in order
+            double segH[8] = {0.0}, segS[8] = {0.0};
+            for (int q = 0; q < 8; ++q)
+                for (int t = tstart[kb] + q; t < tstart[kb + 1]; t += 8) {
+                    segH[q] += pb[(((size_t)t * 2 + 0) * PS + ff) * 32 + lane];
+                    segS[q] += pb[(((size_t)t * 2 + 1) * PS + ff) * 32 + lane];
+                }
+            double sH = segH[0], sS = segS[0];
+            for (int q = 1; q < 8; ++q) {
+                sH += segH[q];
+                sS += segS[q];
             }
             const int lc = m / LCs, ll = m % LCs;
             int kb0 = lc * LCs - 31;
@@ -613,10 +620,17 @@ template <int N> int shard_pairs(const Args &a, const double *x, int LCs, int t0
     for (int ff = 0; ff < PS; ++ff)
         for (int m = 0; m < K; ++m) {
             const int kb = m / 32, lane = m % 32;
-            double sH = 0.0, sS = 0.0;
-            for (int t = std::max(tstart[kb], t0); t < std::min(tstart[kb + 1], t1); ++t) {
-                sH += pb[(((size_t)t * 2 + 0) * PS + ff) * 32 + lane];
-                sS += pb[(((size_t)t * 2 + 1) * PS + ff) * 32 + lane];
+            const int ta = std::max(tstart[kb], t0), tb = std::min(tstart[kb + 1], t1);
+            double segH[8] = {0.0}, segS[8] = {0.0};
+            for (int q = 0; q < 8; ++q)
+                for (int t = ta + q; t < tb; t += 8) {
+                    segH[q] += pb[(((size_t)t * 2 + 0) * PS + ff) * 32 + lane];
+                    segS[q] += pb[(((size_t)t * 2 + 1) * PS + ff) * 32 + lane];
+                }
+            double sH = segH[0], sS = segS[0];
+            for (int q = 1; q < 8; ++q) {
+                sH += segH[q];
+                sS += segS[q];
             }
             const int lc = m / LCs, ll = m % LCs;
             int kb0 = lc * LCs - 31;
