@@ -58,6 +58,10 @@ def parse():
                     help="force the pair pass (auto: the autotuner's choice)")
     ap.add_argument("--no-tune", action="store_true",
                     help="skip the autotuner and use the default tiles (for short profiling runs)")
+    ap.add_argument("--serve-runs", type=int, default=64,
+                    help="truncated-Newton runs (the first of the 256-run serving stream) for the served "
+                         "latency / throughput figures; 0 skips them")
+    ap.add_argument("--serve-maxfun", type=int, default=6, help="evaluations per run of that stream")
     return ap.parse_args()
 
 
@@ -331,6 +335,9 @@ def run_engine(args):
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
         cpu = cpu_port_rate(prob, args.cpu_seconds)
+    served = None
+    if world == 1 and args.serve_runs > 0:
+        served = serving_figures(args.serve_runs, args.serve_maxfun)
     out = {
         "metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
@@ -367,8 +374,31 @@ def run_engine(args):
                          else 8) * args.steps,
         "cpu_baseline": cpu,
         "clocks": clk,
+        "served": served,
     }
     print(json.dumps(out), flush=True)
+
+
+def serving_figures(nruns: int, maxfun: int) -> dict:
+    """The served form on a prefix of the 256-run stream (n uniform over He, H2,
+    LiH; K log-uniform 16-2048; seeds 4000 + j): each run is a truncated-Newton
+    client making at most ``maxfun`` evaluations.  Three ways through the same
+    runs: plain (one after another through the per-call host entry point),
+    served with every run admitted at t = 0 (the capacity), and served with
+    Poisson arrivals at 20/s (the latency figures).  Host wall clock, setup
+    (engine creation, tuning) excluded from plain and from the capacity run."""
+    from nbo_correlatedgaussians_b200 import synth
+    from nbo_correlatedgaussians_b200.loadgen import plain_stream, served_stream
+    probs = synth.workload("serve256")[:nruns]
+    plain = plain_stream(probs, maxfun)
+    sat = served_stream(probs, maxfun, rate=0.0)
+    poi = served_stream(probs, maxfun, rate=20.0, seed=4)
+    keep = ("evals", "wall_s", "evals_per_s", "p50_ms", "p99_ms")
+    return {"workload": f"first {nruns} runs of the 256-run TN stream, maxfun {maxfun}",
+            "plain": {k: plain[k] for k in keep},
+            "served_capacity": {k: sat[k] for k in keep + ("gpu_step_s", "mean_batch")},
+            "served_poisson_20_per_s": {k: poi[k] for k in keep + ("gpu_step_s", "mean_batch")},
+            "capacity_vs_plain": sat["evals_per_s"] / plain["evals_per_s"]}
 
 
 def main():
