@@ -213,6 +213,13 @@ int necg_batch_replay(necg_batch *b, void *stream);
  * first non-OK code or NECG_OK. */
 int necg_batch_status(necg_batch *b, int *status_out, void *stream);
 
+/* The raw status words of the last planned step, without synchronising:
+ * enqueues on `stream` a copy of 2 ints per instance (flags, first failing
+ * pair; flags bit 1 = a pair not positive definite, bit 2 = non-finite) into
+ * flags_host, which should be pinned and is valid once the stream reaches that
+ * point.  For callers that keep several steps in flight. */
+int necg_batch_status_async(necg_batch *b, int *flags_host, void *stream);
+
 /* necg_outprod for callers that cannot allocate device memory (a host that
  * gives the GPU to its own fixed memory pool at start-up, a loop that cannot
  * afford an allocation's implicit synchronisation, a foreign-language driver

@@ -56,6 +56,7 @@ SIGNATURES = [
     ("necg_batch_graph", _i, [_vp, _vp]),
     ("necg_batch_replay", _i, [_vp, _vp]),
     ("necg_batch_status", _i, [_vp, _vp, _vp]),
+    ("necg_batch_status_async", _i, [_vp, _vp, _vp]),
     ("necg_status_string", ctypes.c_char_p, [_i]),
     ("necg_profile", _i, [_vp, _i]),
     ("necg_fp64_peak", _i, [_i, _dp, _vp]),

@@ -63,6 +63,21 @@ class Batch:
         else:
             _lib.check(self.L.necg_batch_step(self.b, s), "necg_batch_step")
 
+    def status_async(self, flags_host, stream=None) -> None:
+        """Enqueue a copy of the last step's raw status words (2 ints per
+        instance) into the pinned int32 tensor ``flags_host``."""
+        _lib.check(self.L.necg_batch_status_async(self.b, ctypes.c_void_p(flags_host.data_ptr()), _stream_ptr(stream)),
+                   "necg_batch_status_async")
+
+    @staticmethod
+    def decode(flags) -> list[int]:
+        """Status codes from raw flag words (as necg_batch_status returns them)."""
+        out = []
+        for fl in flags:
+            fl = int(fl)
+            out.append(_lib.NECG_ERR_NOT_PD if fl & 1 else _lib.NECG_ERR_NONFINITE if fl & 2 else _lib.NECG_OK)
+        return out
+
     def status(self, stream=None) -> list[int]:
         out = (ctypes.c_int * max(1, self.count))()
         self.L.necg_batch_status(self.b, out, _stream_ptr(stream))
@@ -120,6 +135,21 @@ class BatchEngine:
     def step(self, graph: bool = True, stream=None) -> None:
         """Launch one energy+gradient step of the current plan (asynchronous)."""
         self.batch.step(graph, stream)
+
+    def status_async(self, flags_host, stream=None) -> None:
+        """Enqueue a copy of the last step's raw status words (2 ints per
+        instance) into the pinned int32 tensor ``flags_host``."""
+        _lib.check(self.L.necg_batch_status_async(self.b, ctypes.c_void_p(flags_host.data_ptr()), _stream_ptr(stream)),
+                   "necg_batch_status_async")
+
+    @staticmethod
+    def decode(flags) -> list[int]:
+        """Status codes from raw flag words (as necg_batch_status returns them)."""
+        out = []
+        for fl in flags:
+            fl = int(fl)
+            out.append(_lib.NECG_ERR_NOT_PD if fl & 1 else _lib.NECG_ERR_NONFINITE if fl & 2 else _lib.NECG_OK)
+        return out
 
     def status(self, stream=None) -> list[int]:
         return self.batch.status(stream)

@@ -67,6 +67,7 @@ struct PlanPtrs {
     int *order;     // instances by decreasing tile cost (fused queue order)
     int4 *etiles;   // (inst, kb, lc, 0); fused mode: (inst, kb, lc, tile index in the instance)
     int4 *gtiles;
+    int *status_all;  // device only: every instance's status word pair, gathered after the step
 };
 
 __device__ __forceinline__ int find_inst(const int *pref, int ninst, int i) {
@@ -198,6 +199,15 @@ __global__ void __launch_bounds__(256) batch_fsum_kernel(PlanPtrs p) {
         double v = 0.0;
         BATCH_SWITCH(d.n, v = fsym_sum_one<N>(d.stile_start, d.lc_s, d.K, f, m, part_b, part_k, d.scal[0]));
         d.part[(size_t)f * d.K + m] = v;
+    }
+}
+
+// Every instance's status word pair into one array, so one copy reads them all.
+__global__ void batch_status_kernel(PlanPtrs p) {
+    const int ninst = p.hdr->ninst;
+    for (int q = threadIdx.x; q < ninst; q += blockDim.x) {
+        p.status_all[2 * q] = p.inst[q].status[0];
+        p.status_all[2 * q + 1] = p.inst[q].status[1];
     }
 }
 
@@ -393,6 +403,8 @@ void layout(necg_batch *b, char *base, PlanPtrs &p, size_t *total) {
     off = align_up(off + sizeof(int4) * b->cap_tiles, 256);
     p.gtiles = (int4 *)(base + off);
     off = align_up(off + sizeof(int4) * b->cap_tiles, 256);
+    p.status_all = (int *)(base + off);
+    off = align_up(off + sizeof(int) * 2 * b->cap_inst, 256);
     if (total) *total = off;
 }
 
@@ -414,6 +426,7 @@ void launch_step(necg_batch *b, cudaStream_t st, bool fused) {
         batch_sum_kernel<<<g * 4, 256, 0, st>>>(p);
     }
     batch_reduce_kernel<<<g * 2, 128, 0, st>>>(p);
+    batch_status_kernel<<<1, 256, 0, st>>>(p);
 }
 
 int capture(necg_batch *b, int mode) {
@@ -633,6 +646,15 @@ int necg_batch_replay(necg_batch *b, void *stream) {
         if (rc) return rc;
     }
     BCK(cudaGraphLaunch(b->exec[mode], (cudaStream_t)stream));
+    return NECG_OK;
+}
+
+int necg_batch_status_async(necg_batch *b, int *flags_host, void *stream) {
+    if (!b || (b->ninst > 0 && !flags_host)) return NECG_ERR_ARG;
+    BCK(cudaSetDevice(b->device));
+    if (b->ninst > 0)
+        BCK(cudaMemcpyAsync(flags_host, b->ptrs.status_all, sizeof(int) * 2 * b->ninst, cudaMemcpyDeviceToHost,
+                            (cudaStream_t)stream));
     return NECG_OK;
 }
 

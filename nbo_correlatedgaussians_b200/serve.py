@@ -10,10 +10,11 @@ the reference's optimiser, python/necg.py:159-171 and source/tn.f).  The server:
 * admits runs under an HBM budget and a slot count: a run that does not fit
   waits until earlier runs close and free their workspace;
 * batches continuously: a worker thread takes every request that is ready,
-  plans one batched step over those runs (all their energy and gradient tiles
-  in two flattened queues) and launches it as a CUDA-graph replay.  Requests
-  that arrive while a step is on the GPU go into the next step; two batch
-  plans are used alternately, so the host plans step i+1 while step i runs.
+  plans one batched step over those runs (all their tiles in one flattened
+  queue) and launches it as a CUDA-graph replay.  Requests that arrive while a
+  step is on the GPU go into the next step, which is launched at once behind
+  it: two batch plans are used alternately, so up to two steps are in flight
+  and the GPU does not wait for the host to deliver results.
 * reports per-request latency (submit to result) and throughput.
 
 Because every run's tiles and reductions are the same in any batch, a run's
@@ -111,6 +112,7 @@ class Server:
     def start(self) -> "Server":
         self.stream = torch.cuda.Stream(device=self.device)
         self.batches = [Batch(self.max_slots, self.max_tiles), Batch(self.max_slots, self.max_tiles)]
+        self.flags = [torch.zeros(2 * self.max_slots, dtype=torch.int32).pin_memory() for _ in range(2)]
         self.t_start = time.perf_counter()
         self._thread = threading.Thread(target=self._loop, name="necg-server", daemon=True)
         self._thread.start()
@@ -217,32 +219,42 @@ class Server:
 
     # -------------------------------------------------------------- worker
     def _loop(self) -> None:
-        in_flight = None  # (requests, event)
+        """Launch a step as soon as requests are ready, with up to two steps in
+        flight (one per batch plan), and deliver each step when its event has
+        completed; so clients' responses overlap the GPU's work on the other
+        step."""
+        flights: collections.deque = collections.deque()  # (requests, event, batch, timing)
         wave = 0
         with torch.cuda.device(self.device):
             while True:
+                reqs = []
                 with self.lock:
-                    while not self.pending and in_flight is None and not self._stop:
-                        self.lock.wait()
-                    if self._stop and not self.pending and in_flight is None:
-                        return
-                    # at most one request per run per step (runs issue back to back)
-                    reqs, seen, rest = [], set(), collections.deque()
-                    while self.pending:
-                        r = self.pending.popleft()
-                        if r.run.id in seen:
-                            rest.append(r)
-                        else:
-                            seen.add(r.run.id)
-                            reqs.append(r)
-                    self.pending = rest
-                new_flight = None
+                    while True:
+                        if self._stop and not self.pending and not flights:
+                            return
+                        if self.pending and len(flights) < 2:
+                            break
+                        if flights and flights[0][1].query():
+                            break
+                        # nothing to launch or deliver yet: sleep until a request
+                        # arrives, polling the in-flight step meanwhile
+                        self.lock.wait(timeout=2e-4 if flights else None)
+                    if self.pending and len(flights) < 2:
+                        # at most one request per run per step (runs issue back to back)
+                        seen, rest = set(), collections.deque()
+                        while self.pending:
+                            r = self.pending.popleft()
+                            if r.run.id in seen:
+                                rest.append(r)
+                            else:
+                                seen.add(r.run.id)
+                                reqs.append(r)
+                        self.pending = rest
                 if reqs:
-                    new_flight = self._launch(reqs, self.batches[wave % 2])
+                    flights.append(self._launch(reqs, self.batches[wave % 2]))
                     wave += 1
-                if in_flight is not None:
-                    self._deliver(*in_flight)
-                in_flight = new_flight
+                while flights and flights[0][1].query():
+                    self._deliver(*flights.popleft())
 
     def _launch(self, reqs: list[Request], batch: Batch):
         s = self.stream
@@ -260,6 +272,8 @@ class Server:
             e0.record(s)
             batch.step(self.graph, stream=s)
             e1.record(s)
+            flags = self.flags[self.batches.index(batch)]
+            batch.status_async(flags, stream=s)
             for u in runs:
                 u.gh.copy_(u.g, non_blocking=True)
                 u.fh.copy_(u.f, non_blocking=True)
@@ -267,12 +281,12 @@ class Server:
             ev.record(s)
         self.steps += 1
         self.step_sizes.append(len(reqs))
-        return reqs, ev, batch, (e0, e1)
+        return reqs, ev, flags, (e0, e1)
 
-    def _deliver(self, reqs: list[Request], ev, batch: Batch, timing) -> None:
+    def _deliver(self, reqs: list[Request], ev, flags, timing) -> None:
         ev.synchronize()
         self.gpu_ms += timing[0].elapsed_time(timing[1])
-        codes = batch.status(stream=self.stream)
+        codes = Batch.decode(flags[0:2 * len(reqs):2].tolist())
         now = time.perf_counter()
         for r, code in zip(reqs, codes):
             if code == _lib.NECG_ERR_NOT_PD:
