@@ -113,6 +113,7 @@ class Server:
         self.stream = torch.cuda.Stream(device=self.device)
         self.batches = [Batch(self.max_slots, self.max_tiles), Batch(self.max_slots, self.max_tiles)]
         self.flags = [torch.zeros(2 * self.max_slots, dtype=torch.int32).pin_memory() for _ in range(2)]
+        self.free_batches = collections.deque([0, 1])  # plans not in flight
         self.t_start = time.perf_counter()
         self._thread = threading.Thread(target=self._loop, name="necg-server", daemon=True)
         self._thread.start()
@@ -219,44 +220,48 @@ class Server:
 
     # -------------------------------------------------------------- worker
     def _loop(self) -> None:
-        """Launch a step as soon as requests are ready, with up to two steps in
-        flight (one per batch plan), and deliver each step when its event has
-        completed; so clients' responses overlap the GPU's work on the other
-        step."""
-        flights: collections.deque = collections.deque()  # (requests, event, batch, timing)
-        wave = 0
+        """Launch a step as soon as requests are ready and a batch plan is free
+        (two plans: up to two steps in flight).  A watcher thread waits for each
+        step's completion with the GIL released and delivers its results, so
+        clients' responses overlap the GPU's work on the other step and nothing
+        polls."""
+        import queue
+        done_q: queue.Queue = queue.Queue()
+        watcher = threading.Thread(target=self._watch, args=(done_q,), name="necg-deliver", daemon=True)
+        watcher.start()
         with torch.cuda.device(self.device):
             while True:
                 reqs = []
                 with self.lock:
-                    while True:
-                        if self._stop and not self.pending and not flights:
-                            return
-                        if self.pending and len(flights) < 2:
-                            break
-                        if flights and flights[0][1].query():
-                            break
-                        # nothing to launch or deliver yet: sleep until a request
-                        # arrives, polling the in-flight step meanwhile
-                        self.lock.wait(timeout=2e-4 if flights else None)
-                    if self.pending and len(flights) < 2:
-                        # at most one request per run per step (runs issue back to back)
-                        seen, rest = set(), collections.deque()
-                        while self.pending:
-                            r = self.pending.popleft()
-                            if r.run.id in seen:
-                                rest.append(r)
-                            else:
-                                seen.add(r.run.id)
-                                reqs.append(r)
-                        self.pending = rest
-                if reqs:
-                    flights.append(self._launch(reqs, self.batches[wave % 2]))
-                    wave += 1
-                while flights and flights[0][1].query():
-                    self._deliver(*flights.popleft())
+                    while not (self.pending and self.free_batches) and not (self._stop and not self.pending):
+                        self.lock.wait()
+                    if self._stop and not self.pending:
+                        break
+                    # at most one request per run per step (runs issue back to back)
+                    seen, rest = set(), collections.deque()
+                    while self.pending:
+                        r = self.pending.popleft()
+                        if r.run.id in seen:
+                            rest.append(r)
+                        else:
+                            seen.add(r.run.id)
+                            reqs.append(r)
+                    self.pending = rest
+                    bi = self.free_batches.popleft()
+                done_q.put(self._launch(reqs, bi))
+        done_q.put(None)
+        watcher.join()
 
-    def _launch(self, reqs: list[Request], batch: Batch):
+    def _watch(self, done_q) -> None:
+        with torch.cuda.device(self.device):
+            while True:
+                flight = done_q.get()
+                if flight is None:
+                    return
+                self._deliver(*flight)
+
+    def _launch(self, reqs: list[Request], bi: int):
+        batch = self.batches[bi]
         s = self.stream
         with torch.cuda.stream(s):
             for r in reqs:
@@ -272,7 +277,7 @@ class Server:
             e0.record(s)
             batch.step(self.graph, stream=s)
             e1.record(s)
-            flags = self.flags[self.batches.index(batch)]
+            flags = self.flags[bi]
             batch.status_async(flags, stream=s)
             for u in runs:
                 u.gh.copy_(u.g, non_blocking=True)
@@ -281,12 +286,12 @@ class Server:
             ev.record(s)
         self.steps += 1
         self.step_sizes.append(len(reqs))
-        return reqs, ev, flags, (e0, e1)
+        return reqs, ev, bi, (e0, e1)
 
-    def _deliver(self, reqs: list[Request], ev, flags, timing) -> None:
+    def _deliver(self, reqs: list[Request], ev, bi: int, timing) -> None:
         ev.synchronize()
         self.gpu_ms += timing[0].elapsed_time(timing[1])
-        codes = Batch.decode(flags[0:2 * len(reqs):2].tolist())
+        codes = Batch.decode(self.flags[bi][0:2 * len(reqs):2].tolist())
         now = time.perf_counter()
         for r, code in zip(reqs, codes):
             if code == _lib.NECG_ERR_NOT_PD:
@@ -301,6 +306,9 @@ class Server:
             self.latencies.append(now - r.t_submit)
             self.evals_done += 1
             r.done.set()
+        with self.lock:
+            self.free_batches.append(bi)
+            self.lock.notify_all()
 
     # ------------------------------------------------------------ metrics
     def stats(self) -> dict:

@@ -103,3 +103,22 @@ def test_driver_main_oldquit(torch_cuda, tmp_path):
     assert abs(en1[0] - d["en1"][0]) < 1e-9 and normwise(en1, d["en1"]) < 1e-8
     assert np.max(np.abs(res["dipole"] - d["dipole"])) < 1e-7
     assert (tmp_path / "necg.out").read_text().strip().endswith("gmt")
+
+
+def test_driver_tnc_oldquit(torch_cuda, tmp_path):
+    """The driver with SciPy's truncated Newton (at most 50 iterations) from the
+    reference's start point: the reference's own run (through its outprod)
+    converged in 34 iterations; the same count and optimum here."""
+    from nbo_correlatedgaussians_b200 import problem as pr
+    from nbo_correlatedgaussians_b200.necg import main
+    d = golden("driver_tnc_oldquit.npz")
+    p = problem_from(golden("oldquit.npz"))
+    path = tmp_path / "oldquit.dat"
+    pr.write_oldquit(p, str(path))
+    res = main(str(path), maxiter=int(d["maxiter"]), output=str(tmp_path / "necg.out"), method="TNC")
+    assert res["nit"] == int(d["nit"])
+    assert abs(res["f_opt"] - float(d["f_opt"])) < 1e-9
+    x = res["x_opt"].copy()
+    K = p.K
+    x[K * p.blk:] *= np.sign(x[K * p.blk:] @ d["x_opt"][K * p.blk:])
+    assert normwise(x, d["x_opt"]) < 1e-7
