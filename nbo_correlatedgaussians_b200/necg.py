@@ -90,16 +90,24 @@ class _IterationCap(Exception):
     pass
 
 
-def optimise(fun, x0: np.ndarray, method: str = "L-BFGS-B", maxiter: int = 20, nvar: int | None = None):
+def optimise(fun, x0: np.ndarray, method: str = "L-BFGS-B", maxiter: int = 20, nvar: int | None = None,
+             hessp=None):
     """Minimise fun (returning (f, g)) from x0.  L-BFGS-B with the options of
-    python/necg.py:159-171; or "TNC" (SciPy's truncated Newton, the analogue of
+    python/necg.py:159-171; "TNC" (SciPy's truncated Newton, the analogue of
     the Fortran driver's LMQN, source/tn.f) stopped after ``maxiter``
-    iterations.  Returns (x, f, nit, message)."""
+    iterations; or "Newton-CG" with ``hessp(x, v)`` (the Hessian-vector product
+    of the truncated-Newton inner loop, source/tn.f:1301-1327).  Returns (x, f,
+    nit, message)."""
     eps = 2.220446649250313e-16
     nvar = nvar or x0.size
     if method == "L-BFGS-B":
         r = minimize(fun, x0, method="L-BFGS-B", jac=True,
                      options={"maxiter": maxiter, "maxfun": 150 * nvar, "ftol": eps, "gtol": np.sqrt(eps)})
+        return r.x, float(r.fun), int(r.nit), str(r.message)
+    if method == "Newton-CG":
+        if hessp is None:
+            raise ValueError("Newton-CG needs hessp")
+        r = minimize(fun, x0, method="Newton-CG", jac=True, hessp=hessp, options={"maxiter": maxiter})
         return r.x, float(r.fun), int(r.nit), str(r.message)
     if method != "TNC":
         raise ValueError(f"unknown method {method!r}")
@@ -119,11 +127,21 @@ def optimise(fun, x0: np.ndarray, method: str = "L-BFGS-B", maxiter: int = 20, n
         return last["x"], float(f), last["it"], f"stopped after {maxiter} iterations"
 
 
+def write_restart(filename: str) -> None:
+    """The current basis (iv, C) and problem in the oldquit.dat layout, so a run
+    can resume from it (the restart writer of the Fortran driver,
+    source/btn.f:335-363, kept there as a comment)."""
+    from .problem import write_oldquit
+    write_oldquit(_state.problem_from_shared(), filename)
+
+
 def main(input_file: str = "oldquit.dat", maxiter: int = 20, output: str | None = None,
-         method: str = "L-BFGS-B") -> dict:
+         method: str = "L-BFGS-B", restart: str | None = None) -> dict:
     """Run the driver; returns the quantities it prints (for tests and callers).
     method "L-BFGS-B" is python/necg.py's optimiser; "TNC" runs ``maxiter``
-    truncated-Newton iterations instead."""
+    truncated-Newton iterations instead; "Newton-CG" uses Hessian-vector
+    products from two gradients evaluated in one batched step.  ``restart``:
+    write the optimised basis there in the oldquit.dat layout."""
     if output is None:
         output = "necg.out"
     from . import utils
@@ -172,8 +190,16 @@ def main(input_file: str = "oldquit.dat", maxiter: int = 20, output: str | None 
         fvals.append(f)
         return f, g
 
+    hv = None
+    if method == "Newton-CG":
+        from .hessian import HessianVector
+        hv = HessianVector(_state.problem_from_shared())
     t0 = time.perf_counter()
-    x_opt, f_opt, nit, message = optimise(fun, hiv, method, maxiter, sh.siv + sh.M)
+    x_opt, f_opt, nit, message = optimise(fun, hiv, method, maxiter, sh.siv + sh.M,
+                                          hessp=(lambda x, v: hv(x, v)) if hv else None)
+    if hv is not None:
+        res["hessp_calls"] = hv.count
+        hv.close()
     res["t_optimise"] = time.perf_counter() - t0
     print(f"Time for energy/gradient calc. is {res['t_optimise']:.3f} seconds")
     print(f"Energy is {f_opt:.15f} hartree")
@@ -188,6 +214,8 @@ def main(input_file: str = "oldquit.dat", maxiter: int = 20, output: str | None 
     print()
     print("***** End Output Vectors *****")
     print()
+    if restart:
+        write_restart(restart)
     _build_matrices()
     res["en1"] = _rayleigh_quotient()
     _print_energetics(*res["en1"])

@@ -121,3 +121,42 @@ def test_driver_tnc_oldquit(torch_cuda, tmp_path):
     res = main(str(path), maxiter=int(d["maxiter"]), output=str(tmp_path / "necg.out"), method="TNC")
     assert res["nit"] < int(d["maxiter"])  # converged before the cap, as the reference did
     assert abs(res["f_opt"] - float(d["f_opt"])) < 1e-6
+
+
+def test_hessian_vector_batched(torch_cuda):
+    """H v from two gradients in one batched step against central differences of
+    the oracle's gradient, and symmetry u.(H v) = v.(H u)."""
+    from nbo_correlatedgaussians_b200 import synth
+    from nbo_correlatedgaussians_b200.hessian import HessianVector
+    p = synth.make_problem("H2", 24, 41)
+    p.C = np.random.default_rng(4).normal(size=p.K)
+    hv = HessianVector(p, tune=False)
+    rng = np.random.default_rng(9)
+    u, v = rng.normal(size=p.x.size), rng.normal(size=p.x.size)
+    Hv = hv(p.x, v)
+    Hu = hv(p.x, u)
+    o = Oracle.from_problem(p)
+    e = 1e-5 * (1.0 + np.linalg.norm(p.x)) / np.linalg.norm(v)
+    ref = (o.outprod(p.x + e * v, nthreads=8)[1] - o.outprod(p.x - e * v, nthreads=8)[1]) / (2 * e)
+    assert normwise(Hv, ref) < 1e-6
+    assert abs(u @ Hv - v @ Hu) <= 1e-5 * max(abs(u @ Hv), 1e-12)
+    hv.close()
+
+
+def test_driver_newton_cg_and_restart(torch_cuda, tmp_path):
+    """Newton-CG with the batched Hessian-vector product lowers E from the
+    eigenvector start on oldquit.dat, and the restart file reads back to the
+    optimised basis (same E)."""
+    from nbo_correlatedgaussians_b200 import problem as pr
+    from nbo_correlatedgaussians_b200.engine import Engine
+    from nbo_correlatedgaussians_b200.necg import main
+    p = problem_from(golden("oldquit.npz"))
+    path = tmp_path / "oldquit.dat"
+    pr.write_oldquit(p, str(path))
+    rst = tmp_path / "newquit.dat"
+    res = main(str(path), maxiter=5, output=str(tmp_path / "necg.out"), method="Newton-CG", restart=str(rst))
+    assert res["f_opt"] < res["en0"][0] - 1e-3 and res["hessp_calls"] > 0
+    q = pr.read_oldquit(str(rst))
+    assert np.array_equal(q.x, res["x_opt"])
+    f, _ = Engine(q).outprod(q.x)
+    assert abs(f - res["f_opt"]) < TOL_E
