@@ -81,8 +81,9 @@ int necg_set_variant(necg_handle *h, int minw_energy, int minw_grad);
  * set closed under inverse (each sml and sms has its inverse in the set) and
  * n <= 5; otherwise NECG_ERR_UNSUPPORTED.  lc: kets per tile (1..64); minw: 8,
  * 12 or 16 warps per SM, and for mode 2 also 108 and 112 (8 and 12 warps with
- * the ket records re-read at each use instead of held in registers).  Set by
- * the autotuner. */
+ * the ket records re-read at each use instead of held in registers) and 208
+ * (as 108, with the 8 warps of an SM in one block stepping through their terms
+ * together).  Set by the autotuner. */
 int necg_set_symmetric(necg_handle *h, int mode, int lc, int minw);
 
 /* One objective evaluation: python/outprod.py:20-76 outprod(x) -> (f, g),

@@ -59,7 +59,7 @@ void free_all(necg_handle *h) {
     void *ptrs[] = {h->d_sml, h->d_sms, h->d_scvv, h->d_bra, h->d_ket, h->d_part, h->d_H,
                     h->d_S, h->d_rows, h->d_scal, h->d_x, h->d_g, h->d_f, h->d_status,
                     h->d_tiles, h->d_pinv, h->d_kcnt, h->d_ksrc, h->d_kcoef, h->d_stiles,
-                    h->d_stile_start, h->d_psym};
+                    h->d_stile_start, h->d_psym, h->d_sgroups, h->d_qcount};
     for (void *p : ptrs)
         if (p) cudaFree(p);
 }
@@ -119,6 +119,20 @@ int ensure_sym_tiles(necg_handle *h, int K, cudaStream_t st, int mult) {
         h->ws_bytes += (long long)((need - h->psym_cap) * sizeof(double));
         h->psym_cap = need;
     }
+    std::vector<int2> groups;  // 8 consecutive ket chunks of one row block, largest blocks first
+    for (int kb = nkb - 1; kb >= 0; --kb) {
+        const int ntk = start[kb + 1] - start[kb];
+        for (int lc0 = 0; lc0 < ntk; lc0 += 8) groups.push_back(make_int2(kb, lc0));
+    }
+    if ((int)groups.size() > h->sgroups_cap) {
+        if (h->d_sgroups) cudaFree(h->d_sgroups);
+        h->d_sgroups = nullptr;
+        CK(cudaMalloc((void **)&h->d_sgroups, groups.size() * sizeof(int2)));
+        h->sgroups_cap = (int)groups.size();
+    }
+    if (!h->d_qcount) CK(cudaMalloc((void **)&h->d_qcount, sizeof(int)));
+    CK(cudaMemcpyAsync(h->d_sgroups, groups.data(), groups.size() * sizeof(int2), cudaMemcpyHostToDevice, st));
+    h->nsgroups = (int)groups.size();
     CK(cudaMemcpyAsync(h->d_stiles, t.data(), t.size() * sizeof(int2), cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(h->d_stile_start, start.data(), start.size() * sizeof(int), cudaMemcpyHostToDevice, st));
     CK(cudaStreamSynchronize(st));
@@ -245,6 +259,9 @@ LaunchArgs base_args(necg_handle *h, int K) {
     a.LC_s = h->lc_s;
     a.minb_s = h->minb_s;
     a.psym = h->d_psym;
+    a.sgroups = h->d_sgroups;
+    a.nsgroups = h->nsgroups;
+    a.qcount = h->d_qcount;
     return a;
 }
 
@@ -371,7 +388,7 @@ int necg_set_tiles(necg_handle *h, int lc_energy, int lc_grad) {
 }
 
 int necg_set_symmetric(necg_handle *h, int mode, int lc, int minw) {
-    const bool okw = minw == 8 || minw == 12 || minw == 16 || (mode == 2 && (minw == 108 || minw == 112));
+    const bool okw = minw == 8 || minw == 12 || minw == 16 || (mode == 2 && (minw == 108 || minw == 112 || minw == 208));
     if (!h || mode < 0 || mode > 2 || lc < 1 || lc > 64 || !okw) return NECG_ERR_ARG;
     if (mode && !h->sym_ok) return NECG_ERR_UNSUPPORTED;
     h->grad_mode = mode;
@@ -434,6 +451,9 @@ int necg_outprod(necg_handle *h, int K, const double *x_dev, double *f_dev, doub
         a.nstiles = h->nstiles;
         a.LC_s = h->lc_s;
         a.psym = h->d_psym;
+        a.sgroups = h->d_sgroups;
+        a.nsgroups = h->nsgroups;
+        a.qcount = h->d_qcount;
         mark(h, 0, st);
         if (necg::launch_prep(a, st)) return NECG_ERR_UNSUPPORTED;
         mark(h, 1, st);

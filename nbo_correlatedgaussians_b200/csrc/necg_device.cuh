@@ -53,13 +53,17 @@ struct FusedSmem {
 // so every lane evaluates a term: a lane without a pair (l > k, or k >= K)
 // evaluates the finite pair (l, l, P) with zero weights, which adds nothing.
 // VKET: ket records re-read at each use (fewer live registers).
-template <int N, bool VKET>
+// BSYNC: the warps of a block step through their tiles' terms together (a
+// block barrier after every (l, P) term, so the warps sharing a scheduler
+// execute the same stretch of code); every warp then runs LC x nst iterations,
+// and an idle warp (no tile: idle = true, or l >= K) only takes the barriers.
+template <int N, bool VKET, bool BSYNC = false>
 __device__ __forceinline__ void fsym_tile(int t, int2 tl, int LC, int K, int nst, const Consts<N> &cs,
                                           const double *__restrict__ bra, const double *__restrict__ ket,
                                           const double *__restrict__ C, const KetMap &kmap,
                                           double *__restrict__ H, double *__restrict__ S,
                                           double *__restrict__ part_b, double *__restrict__ part_k,
-                                          int *status, FusedSmem sm) {
+                                          int *status, FusedSmem sm, bool idle = false) {
     using KL = KetLayout<N>;
     constexpr int PS = Part<N>::size;
     static_assert(PS <= 32, "the symmetric pass needs tri(n) + 1 + 3n <= 32");
@@ -67,8 +71,8 @@ __device__ __forceinline__ void fsym_tile(int t, int2 tl, int LC, int K, int nst
     double *krow0 = sm.krow, *krow1 = sm.krow + 16 * 33, *kred = sm.kred;
     const int k = tl.x * 32 + lane;
     const int l0 = tl.y * LC;
-    const int l1 = min(l0 + LC, K);
-    const bool kval = k < K;
+    const int l1 = BSYNC ? l0 + LC : min(l0 + LC, K);
+    const bool kval = k < K && !idle;
     const double Ck = kval ? C[k] : 0.0;
     SmemAcc<N> accH{sm.sacc + lane}, accS{sm.sacc + PS * 32 + lane};
     accH.zero();
@@ -89,10 +93,16 @@ __device__ __forceinline__ void fsym_tile(int t, int2 tl, int LC, int K, int nst
     bool ok = true;
     int flags = 0, bad = 0;
     for (int l = l0; l < l1; ++l) {
+        // warp-uniform: this (l) has work (always, without BSYNC)
+        const bool lok = !BSYNC || (!idle && l < K);
         double aH = 0.0, aS = 0.0, hsum = 0.0, ssum = 0.0;
-        const bool active = kval && l <= k;
-        const BraRef b{bra + (active ? k : l), (size_t)K};
+        const bool active = kval && l <= k && lok;
+        const BraRef b{bra + (active ? k : (lok ? l : 0)), (size_t)K};
         for (int P = 0; P < nst; ++P) {
+            if (BSYNC && !lok) {
+                __syncthreads();
+                continue;
+            }
             const double *kr = ket + ((size_t)l * nst + P) * KL::size;
             const double wb = active ? kr[KL::wC] : 0.0;
             const double wk = active && l < k ? 2.0 * Ck * kr[KL::winv] : 0.0;
@@ -125,7 +135,9 @@ __device__ __forceinline__ void fsym_tile(int t, int2 tl, int LC, int K, int nst
                 }
                 __syncwarp();
             }
+            if (BSYNC) __syncthreads();
         }
+        if (BSYNC && !lok) continue;
         if (active) {
             if (!isfinite(hsum) || !isfinite(ssum)) {
                 if (!(flags & 2)) bad = k * K + l;

@@ -38,6 +38,9 @@ struct necg_handle {
     int stiles_cap = 0, stiles_K = -1, stiles_lc = -1, nstiles = 0;
     double *d_psym = nullptr;
     size_t psym_cap = 0;  // doubles
+    int2 *d_sgroups = nullptr;  // groups of 8 fused tiles of one row block (kb, first lc)
+    int sgroups_cap = 0, nsgroups = 0;
+    int *d_qcount = nullptr;    // queue head of the block-synchronised fused pass
 };
 
 namespace necg {

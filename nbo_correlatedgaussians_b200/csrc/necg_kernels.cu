@@ -291,6 +291,47 @@ __global__ void __launch_bounds__(32, MINW) fsym_kernel(const int2 *__restrict__
                        FusedSmem{sacc, krow, kred});
 }
 
+// The fused pass with 8-warp blocks, one per SM, persistent over a queue of
+// tile groups: group g = row block kb and ket chunks lc0 .. lc0 + 7, one per
+// warp.  The 8 warps read the same 32 bras and step through their terms
+// together (fsym_tile with BSYNC), so the two warps on each scheduler run the
+// same stretch of the long term body.  Shared memory: each warp's FusedSmem,
+// dynamic (2 PS 32 + 2 16 33 + 32 doubles per warp).
+template <int N, bool VKET>
+__global__ void __launch_bounds__(256, 1) fsym_block_kernel(const int2 *__restrict__ groups, int ngroups,
+                                                         int *__restrict__ qcount,
+                                                         const int *__restrict__ tstart, int LC, int K,
+                                                         int nst, Consts<N> cs,
+                                                         const double *__restrict__ bra,
+                                                         const double *__restrict__ ket,
+                                                         const double *__restrict__ C, KetMap kmap,
+                                                         double *__restrict__ H, double *__restrict__ S,
+                                                         double *__restrict__ part_b,
+                                                         double *__restrict__ part_k, int *status) {
+    extern __shared__ double smem[];
+    __shared__ int gsh;
+    constexpr int PS = Part<N>::size;
+    constexpr int PER_WARP = 2 * PS * 32 + 2 * 16 * 33 + 32;
+    const int w = threadIdx.x >> 5;
+    double *base = smem + w * PER_WARP;
+    const FusedSmem sm{base, base + 2 * PS * 32, base + 2 * PS * 32 + 2 * 16 * 33};
+    for (;;) {
+        if (threadIdx.x == 0) gsh = atomicAdd(qcount, 1);
+        __syncthreads();
+        const int g = gsh;
+        __syncthreads();  // every thread has read gsh before it changes
+        if (g >= ngroups) break;
+        const int2 gr = groups[g];
+        const int kb = gr.x, lc = gr.y + w;
+        const int last = min(kb * 32 + 31, K - 1);
+        const bool idle = lc * LC > last;  // past this block's triangle: barriers only
+        fsym_tile<N, VKET, true>(tstart[kb] + lc, make_int2(kb, lc), LC, K, nst, cs, bra, ket, C, kmap, H, S,
+                                 part_b, part_k, status, sm, idle);
+    }
+}
+
+template <int N> constexpr int fsym_block_smem() { return 8 * (2 * Part<N>::size * 32 + 2 * 16 * 33 + 32) * 8; }
+
 // Sum the fused-pass partials and combine out[f * K + m] = sum_H - E sum_S with
 // E = scal[0] (written by finalize after the pass).  Block (kb, f): the 32
 // bases of row block kb, field f.  Their bra partials come from every tile of
@@ -678,7 +719,31 @@ template <int N> struct Launch {
                 a.psym + (size_t)a.nstiles * 2 * Part<N>::size * 32, a.status);
         }
     }
+    static void fsym_block(const LaunchArgs &a, cudaStream_t st) {
+        if constexpr (Part<N>::size <= 32) {
+            constexpr int smem = fsym_block_smem<N>();
+            static bool attr = false;  // per instantiation; the size is the same on every device
+            if (!attr) {
+                cudaFuncSetAttribute(fsym_block_kernel<N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+                attr = true;
+            }
+            int dev = 0, sms = 148;
+            cudaGetDevice(&dev);
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+            Consts<N> cs = make_consts<N>(a.mass_h, a.ncv_h, a.efs);
+            cudaMemsetAsync(a.qcount, 0, sizeof(int), st);
+            const int grid = a.nsgroups < sms ? a.nsgroups : sms;
+            if (grid < 1) return;
+            fsym_block_kernel<N, true><<<grid, 256, smem, st>>>(
+                a.sgroups, a.nsgroups, a.qcount, a.stile_start, a.LC_s, a.K, a.nst, cs, a.bra, a.ket, a.C, a.kmap,
+                a.H, a.S, a.psym, a.psym + (size_t)a.nstiles * 2 * Part<N>::size * 32, a.status);
+        }
+    }
     static void fsym_tiles(const LaunchArgs &a, cudaStream_t st) {
+        if (a.minb_s == 208 && a.st_end == 0 && a.sgroups && a.qcount) {
+            fsym_block(a, st);
+            return;
+        }
         switch (a.minb_s) {  // 100 + w: ket records read at the point of use
         case 12: fsym_v<12, false>(a, st); break;
         case 16: fsym_v<16, false>(a, st); break;

@@ -31,6 +31,10 @@ struct LaunchArgs {
     // sums (non-null): write the per-basis sums there and stop before GRADA
     int st_begin, st_end;
     double *sums;
+    // block-synchronised fused pass (variant 208): groups of 8 tiles of one row block
+    const int2 *sgroups;                   // (kb, first lc)
+    int nsgroups;
+    int *qcount;                           // group queue head (reset before the launch)
 };
 
 int launch_prep(const LaunchArgs &a, cudaStream_t st);
