@@ -65,7 +65,7 @@ def parse():
     return ap.parse_args()
 
 
-DEFAULT_TILES = {"lc_e": 2, "minb_e": 16, "lc_g": 4, "minb_g": 8, "sym": 2, "lc_s": 2, "minw_s": 108}
+DEFAULT_TILES = {"lc_e": 2, "minb_e": 16, "lc_g": 4, "minb_g": 8, "sym": 2, "lc_s": 2, "minw_s": 208}
 PASS_MODE = {"ordered": 0, "symmetric": 1, "fused": 2}
 
 
