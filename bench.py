@@ -312,7 +312,8 @@ def run_engine(args):
     ph_mean = ph.mean(axis=0)
     energy_flops = unordered * tf["energy"]
     if mode == 2:  # one pass over unordered pairs: H, S and both gradients
-        kname, per_term = f"fsym_kernel<{n}>", "fused"
+        block = int(tiles.get("minw_s", 8)) == 208  # 8-warp lockstep blocks
+        kname, per_term = (f"fsym_block_kernel<{n}>" if block else f"fsym_kernel<{n}>"), "fused"
         kern_flops, kern_ms = unordered * tf["fused"], float(ph_mean[1])
         eval_flops = kern_flops
     elif mode == 1:  # energy pass + unordered pairs with bra and ket gradients
