@@ -39,7 +39,8 @@ MINB = (8, 12, 16, 20)
 MINB_GRAD_EXTRA = (112, 116)  # gradient kernel with shared-memory accumulators
 LC_S = (2, 4, 8, 16)          # kets per tile of the symmetric gradient pass
 MINW_SYM = (8, 12)
-MINW_FUSED = (8, 12, 16, 108, 112, 208)  # 100 + w: ket records re-read at each use; 208: 8-warp lockstep blocks
+MINW_FUSED = (8, 12, 16, 108, 112, 208, 218)  # 100 + w: ket records re-read at each use; 208: 8-warp lockstep
+# blocks; 218: the same with the block's bras staged in shared memory
 
 
 def _bucket(K: int) -> int:

@@ -388,7 +388,7 @@ int necg_set_tiles(necg_handle *h, int lc_energy, int lc_grad) {
 }
 
 int necg_set_symmetric(necg_handle *h, int mode, int lc, int minw) {
-    const bool okw = minw == 8 || minw == 12 || minw == 16 || (mode == 2 && (minw == 108 || minw == 112 || minw == 208));
+    const bool okw = minw == 8 || minw == 12 || minw == 16 || (mode == 2 && (minw == 108 || minw == 112 || minw == 208 || minw == 218));
     if (!h || mode < 0 || mode > 2 || lc < 1 || lc > 64 || !okw) return NECG_ERR_ARG;
     if (mode && !h->sym_ok) return NECG_ERR_UNSUPPORTED;
     h->grad_mode = mode;

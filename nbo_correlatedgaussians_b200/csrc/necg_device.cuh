@@ -57,13 +57,17 @@ struct FusedSmem {
 // block barrier after every (l, P) term, so the warps sharing a scheduler
 // execute the same stretch of code); every warp then runs LC x nst iterations,
 // and an idle warp (no tile: idle = true, or l >= K) only takes the barriers.
-template <int N, bool VKET, bool BSYNC = false>
+// SBRA: the block's 32 bras of row block tl.x are staged in shared memory at
+// sbra (field f of lane j at sbra[f * 32 + j]; rows past K hold row K - 1) and
+// read there instead of from global memory.
+template <int N, bool VKET, bool BSYNC = false, bool SBRA = false>
 __device__ __forceinline__ void fsym_tile(int t, int2 tl, int LC, int K, int nst, const Consts<N> &cs,
                                           const double *__restrict__ bra, const double *__restrict__ ket,
                                           const double *__restrict__ C, const KetMap &kmap,
                                           double *__restrict__ H, double *__restrict__ S,
                                           double *__restrict__ part_b, double *__restrict__ part_k,
-                                          int *status, FusedSmem sm, bool idle = false) {
+                                          int *status, FusedSmem sm, bool idle = false,
+                                          const double *sbra = nullptr) {
     using KL = KetLayout<N>;
     constexpr int PS = Part<N>::size;
     static_assert(PS <= 32, "the symmetric pass needs tri(n) + 1 + 3n <= 32");
@@ -108,7 +112,10 @@ __device__ __forceinline__ void fsym_tile(int t, int2 tl, int LC, int K, int nst
             const double wk = active && l < k ? 2.0 * Ck * kr[KL::winv] : 0.0;
             double h, ov;
             bool tok;
-            if constexpr (VKET)
+            if constexpr (SBRA)
+                tok = term_fused<N, double>(BraSmem{sbra + lane}, KetRefV{kr}, cs, wb, wk, accH, accS, koH, koS, h,
+                                            ov);
+            else if constexpr (VKET)
                 tok = term_fused<N, double>(b, KetRefV{kr}, cs, wb, wk, accH, accS, koH, koS, h, ov);
             else
                 tok = term_fused<N, double>(b, kr, cs, wb, wk, accH, accS, koH, koS, h, ov);

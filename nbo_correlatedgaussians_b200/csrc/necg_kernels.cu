@@ -297,7 +297,7 @@ __global__ void __launch_bounds__(32, MINW) fsym_kernel(const int2 *__restrict__
 // together (fsym_tile with BSYNC), so the two warps on each scheduler run the
 // same stretch of the long term body.  Shared memory: each warp's FusedSmem,
 // dynamic (2 PS 32 + 2 16 33 + 32 doubles per warp).
-template <int N, bool VKET>
+template <int N, bool VKET, bool SBRA>
 __global__ void __launch_bounds__(256, 1) fsym_block_kernel(const int2 *__restrict__ groups, int ngroups,
                                                          int *__restrict__ qcount,
                                                          const int *__restrict__ tstart, int LC, int K,
@@ -312,8 +312,10 @@ __global__ void __launch_bounds__(256, 1) fsym_block_kernel(const int2 *__restri
     __shared__ int gsh;
     constexpr int PS = Part<N>::size;
     constexpr int PER_WARP = 2 * PS * 32 + 2 * 16 * 33 + 32;
+    constexpr int BS = BraLayout<N>::size;
     const int w = threadIdx.x >> 5;
     double *base = smem + w * PER_WARP;
+    double *sbra = smem + 8 * PER_WARP;  // SBRA: BS x 32 doubles after the 8 warps' areas
     const FusedSmem sm{base, base + 2 * PS * 32, base + 2 * PS * 32 + 2 * 16 * 33};
     for (;;) {
         if (threadIdx.x == 0) gsh = atomicAdd(qcount, 1);
@@ -325,12 +327,22 @@ __global__ void __launch_bounds__(256, 1) fsym_block_kernel(const int2 *__restri
         const int kb = gr.x, lc = gr.y + w;
         const int last = min(kb * 32 + 31, K - 1);
         const bool idle = lc * LC > last;  // past this block's triangle: barriers only
-        fsym_tile<N, VKET, true>(tstart[kb] + lc, make_int2(kb, lc), LC, K, nst, cs, bra, ket, C, kmap, H, S,
-                                 part_b, part_k, status, sm, idle);
+        if constexpr (SBRA) {  // the group's 32 bras, once for all 8 warps
+            for (int i = threadIdx.x; i < BS * 32; i += 256) {
+                const int f = i >> 5, kk = min(kb * 32 + (i & 31), K - 1);
+                sbra[i] = bra[(size_t)f * K + kk];
+            }
+            __syncthreads();
+        }
+        fsym_tile<N, VKET, true, SBRA>(tstart[kb] + lc, make_int2(kb, lc), LC, K, nst, cs, bra, ket, C, kmap, H,
+                                       S, part_b, part_k, status, sm, idle, sbra);
+        if constexpr (SBRA) __syncthreads();  // sbra is rewritten for the next group
     }
 }
 
-template <int N> constexpr int fsym_block_smem() { return 8 * (2 * Part<N>::size * 32 + 2 * 16 * 33 + 32) * 8; }
+template <int N, bool SBRA> constexpr int fsym_block_smem() {
+    return (8 * (2 * Part<N>::size * 32 + 2 * 16 * 33 + 32) + (SBRA ? BraLayout<N>::size * 32 : 0)) * 8;
+}
 
 // Sum the fused-pass partials and combine out[f * K + m] = sum_H - E sum_S with
 // E = scal[0] (written by finalize after the pass).  Block (kb, f): the 32
@@ -719,12 +731,13 @@ template <int N> struct Launch {
                 a.psym + (size_t)a.nstiles * 2 * Part<N>::size * 32, a.status);
         }
     }
-    static void fsym_block(const LaunchArgs &a, cudaStream_t st) {
+    template <bool SBRA> static void fsym_block(const LaunchArgs &a, cudaStream_t st) {
         if constexpr (Part<N>::size <= 32) {
-            constexpr int smem = fsym_block_smem<N>();
+            constexpr int smem = fsym_block_smem<N, SBRA>();
             static bool attr = false;  // per instantiation; the size is the same on every device
             if (!attr) {
-                cudaFuncSetAttribute(fsym_block_kernel<N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+                cudaFuncSetAttribute(fsym_block_kernel<N, true, SBRA>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     smem);
                 attr = true;
             }
             int dev = 0, sms = 148;
@@ -734,14 +747,15 @@ template <int N> struct Launch {
             cudaMemsetAsync(a.qcount, 0, sizeof(int), st);
             const int grid = a.nsgroups < sms ? a.nsgroups : sms;
             if (grid < 1) return;
-            fsym_block_kernel<N, true><<<grid, 256, smem, st>>>(
+            fsym_block_kernel<N, true, SBRA><<<grid, 256, smem, st>>>(
                 a.sgroups, a.nsgroups, a.qcount, a.stile_start, a.LC_s, a.K, a.nst, cs, a.bra, a.ket, a.C, a.kmap,
                 a.H, a.S, a.psym, a.psym + (size_t)a.nstiles * 2 * Part<N>::size * 32, a.status);
         }
     }
     static void fsym_tiles(const LaunchArgs &a, cudaStream_t st) {
-        if (a.minb_s == 208 && a.st_end == 0 && a.sgroups && a.qcount) {
-            fsym_block(a, st);
+        if ((a.minb_s == 208 || a.minb_s == 218) && a.st_end == 0 && a.sgroups && a.qcount) {
+            if (a.minb_s == 218) fsym_block<true>(a, st);
+            else fsym_block<false>(a, st);
             return;
         }
         switch (a.minb_s) {  // 100 + w: ket records read at the point of use

@@ -132,6 +132,17 @@ struct BraRef {
     size_t K;
     __device__ __forceinline__ double operator()(int f) const { return ldv(p + (size_t)f * K); }
 };
+// Bra record staged in shared memory (field f of this lane at p[f * 32]), read
+// at the point of use through a volatile shared load (not hoisted into registers).
+struct BraSmem {
+    const double *p;  // shared base + lane
+    __device__ __forceinline__ double operator()(int f) const {
+        double v;
+        const unsigned a = (unsigned)__cvta_generic_to_shared(p + f * 32);
+        asm volatile("ld.shared.f64 %0, [%1];" : "=d"(v) : "r"(a));
+        return v;
+    }
+};
 // Ket record read at the point of use (warp-uniform, L1 broadcast), so its
 // fields do not stay live in registers between their uses within a term.
 struct KetRefV {

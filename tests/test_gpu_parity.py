@@ -232,7 +232,7 @@ def test_fused_pass_matches_oracle(torch_cuda, system, K, lc):
     assert L.necg_set_symmetric(eng.h, 1, lc, 8) == _lib.NECG_OK
     f1, g1 = eng.outprod(p.x)
     fr, gr, Hr, Sr = Oracle.from_problem(p).outprod(p.x, nthreads=8, return_hs=True)
-    for minw in (8, 12, 16, 108, 112, 208):
+    for minw in (8, 12, 16, 108, 112, 208, 218):
         assert L.necg_set_symmetric(eng.h, 2, lc, minw) == _lib.NECG_OK
         H = torch.empty((K, K), dtype=torch.float64, device=eng.device)
         S = torch.empty_like(H)
