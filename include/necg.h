@@ -83,8 +83,10 @@ int necg_set_variant(necg_handle *h, int minw_energy, int minw_grad);
  * 12 or 16 warps per SM, and for mode 2 also 108 and 112 (8 and 12 warps with
  * the ket records re-read at each use instead of held in registers) and 208
  * (as 108, with the 8 warps of an SM in one block stepping through their terms
- * together) and 218 (as 208, with the block's bra records staged in shared
- * memory).  Set by the autotuner. */
+ * together), 218 (as 208, with the block's bra records staged in shared
+ * memory), 228 (as 218, each warp's current ket record staged too), 222 and 232
+ * (218 and 228 with 12 warps per block; NECG_ERR_UNSUPPORTED where their shared
+ * memory does not fit, n = 5).  Set by the autotuner. */
 int necg_set_symmetric(necg_handle *h, int mode, int lc, int minw);
 
 /* One objective evaluation: python/outprod.py:20-76 outprod(x) -> (f, g),

@@ -39,8 +39,11 @@ MINB = (8, 12, 16, 20)
 MINB_GRAD_EXTRA = (112, 116)  # gradient kernel with shared-memory accumulators
 LC_S = (2, 4, 8, 16)          # kets per tile of the symmetric gradient pass
 MINW_SYM = (8, 12)
-MINW_FUSED = (8, 12, 16, 108, 112, 208, 218)  # 100 + w: ket records re-read at each use; 208: 8-warp lockstep
-# blocks; 218: the same with the block's bras staged in shared memory
+MINW_FUSED = (8, 12, 16, 108, 112, 208, 218, 228, 222, 232)
+# 100 + w: ket records re-read at each use; 2xy: lockstep blocks (208 8 warps,
+# 218 + bras in shared memory, 228 + ket record in shared memory, 222 / 232 the
+# same with 12 warps); a variant whose shared memory does not fit for n is refused
+# by necg_set_symmetric and skipped
 
 
 def _bucket(K: int) -> int:
@@ -125,7 +128,8 @@ def tune(eng: Engine, x, K: int, reps: int = 3, report: bool = False) -> dict:
         fused = None
         for minw in MINW_FUSED:
             for lc in LC_S:
-                _lib.check(L.necg_set_symmetric(eng.h, 2, lc, minw), "necg_set_symmetric")
+                if L.necg_set_symmetric(eng.h, 2, lc, minw) != _lib.NECG_OK:
+                    continue
                 _phase_times(eng, x, K, 1)
                 t = _phase_times(eng, x, K, reps).min(axis=0)
                 tot = float(t[1] + t[3] + t[4])

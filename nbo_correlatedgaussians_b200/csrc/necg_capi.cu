@@ -92,7 +92,8 @@ int ensure_tiles(necg_handle *h, int K, cudaStream_t st) {
 // mult = 2 for the fused pass (H and S partials kept apart), 1 otherwise.
 int ensure_sym_tiles(necg_handle *h, int K, cudaStream_t st, int mult) {
     const int PS = necg::part_stride(h->n);
-    if (h->stiles_K == K && h->stiles_lc == h->lc_s &&
+    const int gw = necg::fused_block_warps(h->minb_s);  // tiles per group of the lockstep-block pass
+    if (h->stiles_K == K && h->stiles_lc == h->lc_s && h->sgroups_w == gw &&
         (size_t)h->nstiles * PS * (32 + h->lc_s) * mult <= h->psym_cap)
         return NECG_OK;
     std::vector<int2> t;
@@ -119,10 +120,10 @@ int ensure_sym_tiles(necg_handle *h, int K, cudaStream_t st, int mult) {
         h->ws_bytes += (long long)((need - h->psym_cap) * sizeof(double));
         h->psym_cap = need;
     }
-    std::vector<int2> groups;  // 8 consecutive ket chunks of one row block, largest blocks first
+    std::vector<int2> groups;  // gw consecutive ket chunks of one row block, largest blocks first
     for (int kb = nkb - 1; kb >= 0; --kb) {
         const int ntk = start[kb + 1] - start[kb];
-        for (int lc0 = 0; lc0 < ntk; lc0 += 8) groups.push_back(make_int2(kb, lc0));
+        for (int lc0 = 0; lc0 < ntk; lc0 += gw) groups.push_back(make_int2(kb, lc0));
     }
     if ((int)groups.size() > h->sgroups_cap) {
         if (h->d_sgroups) cudaFree(h->d_sgroups);
@@ -133,6 +134,7 @@ int ensure_sym_tiles(necg_handle *h, int K, cudaStream_t st, int mult) {
     if (!h->d_qcount) CK(cudaMalloc((void **)&h->d_qcount, sizeof(int)));
     CK(cudaMemcpyAsync(h->d_sgroups, groups.data(), groups.size() * sizeof(int2), cudaMemcpyHostToDevice, st));
     h->nsgroups = (int)groups.size();
+    h->sgroups_w = gw;
     CK(cudaMemcpyAsync(h->d_stiles, t.data(), t.size() * sizeof(int2), cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(h->d_stile_start, start.data(), start.size() * sizeof(int), cudaMemcpyHostToDevice, st));
     CK(cudaStreamSynchronize(st));
@@ -388,8 +390,10 @@ int necg_set_tiles(necg_handle *h, int lc_energy, int lc_grad) {
 }
 
 int necg_set_symmetric(necg_handle *h, int mode, int lc, int minw) {
-    const bool okw = minw == 8 || minw == 12 || minw == 16 || (mode == 2 && (minw == 108 || minw == 112 || minw == 208 || minw == 218));
+    const bool blockv = minw == 208 || minw == 218 || minw == 228 || minw == 222 || minw == 232;
+    const bool okw = minw == 8 || minw == 12 || minw == 16 || (mode == 2 && (minw == 108 || minw == 112 || blockv));
     if (!h || mode < 0 || mode > 2 || lc < 1 || lc > 64 || !okw) return NECG_ERR_ARG;
+    if (blockv && !necg::fused_variant_ok(h->n, minw)) return NECG_ERR_UNSUPPORTED;  // shared memory
     if (mode && !h->sym_ok) return NECG_ERR_UNSUPPORTED;
     h->grad_mode = mode;
     h->lc_s = lc;

@@ -35,6 +35,7 @@ __device__ __forceinline__ void flag_status(int *status, int flags, int pair) {
 // reduction row (32).  Sized by the caller for its largest n.
 struct FusedSmem {
     double *sacc, *krow, *kred;
+    double *sket;  // SKET: this warp's copy of the current ket record
 };
 
 // One tile of the fused pass over unordered pairs (k >= l): the symmetric
@@ -60,7 +61,9 @@ struct FusedSmem {
 // SBRA: the block's 32 bras of row block tl.x are staged in shared memory at
 // sbra (field f of lane j at sbra[f * 32 + j]; rows past K hold row K - 1) and
 // read there instead of from global memory.
-template <int N, bool VKET, bool BSYNC = false, bool SBRA = false>
+// SKET: each (l, P) ket record is copied by the warp into sm.sket and read
+// there.
+template <int N, bool VKET, bool BSYNC = false, bool SBRA = false, bool SKET = false>
 __device__ __forceinline__ void fsym_tile(int t, int2 tl, int LC, int K, int nst, const Consts<N> &cs,
                                           const double *__restrict__ bra, const double *__restrict__ ket,
                                           const double *__restrict__ C, const KetMap &kmap,
@@ -108,11 +111,18 @@ __device__ __forceinline__ void fsym_tile(int t, int2 tl, int LC, int K, int nst
                 continue;
             }
             const double *kr = ket + ((size_t)l * nst + P) * KL::size;
+            if constexpr (SKET) {
+                for (int i = lane; i < KL::size; i += 32) sm.sket[i] = kr[i];
+                __syncwarp();
+            }
             const double wb = active ? kr[KL::wC] : 0.0;
             const double wk = active && l < k ? 2.0 * Ck * kr[KL::winv] : 0.0;
             double h, ov;
             bool tok;
-            if constexpr (SBRA)
+            if constexpr (SBRA && SKET)
+                tok = term_fused<N, double>(BraSmem{sbra + lane}, KetSmem{sm.sket}, cs, wb, wk, accH, accS, koH, koS,
+                                            h, ov);
+            else if constexpr (SBRA)
                 tok = term_fused<N, double>(BraSmem{sbra + lane}, KetRefV{kr}, cs, wb, wk, accH, accS, koH, koS, h,
                                             ov);
             else if constexpr (VKET)

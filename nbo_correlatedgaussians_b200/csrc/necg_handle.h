@@ -39,7 +39,7 @@ struct necg_handle {
     double *d_psym = nullptr;
     size_t psym_cap = 0;  // doubles
     int2 *d_sgroups = nullptr;  // groups of 8 fused tiles of one row block (kb, first lc)
-    int sgroups_cap = 0, nsgroups = 0;
+    int sgroups_cap = 0, nsgroups = 0, sgroups_w = 0;
     int *d_qcount = nullptr;    // queue head of the block-synchronised fused pass
 };
 

@@ -291,32 +291,42 @@ __global__ void __launch_bounds__(32, MINW) fsym_kernel(const int2 *__restrict__
                        FusedSmem{sacc, krow, kred});
 }
 
-// The fused pass with 8-warp blocks, one per SM, persistent over a queue of
-// tile groups: group g = row block kb and ket chunks lc0 .. lc0 + 7, one per
-// warp.  The 8 warps read the same 32 bras and step through their terms
-// together (fsym_tile with BSYNC), so the two warps on each scheduler run the
-// same stretch of the long term body.  Shared memory: each warp's FusedSmem,
-// dynamic (2 PS 32 + 2 16 33 + 32 doubles per warp).
-template <int N, bool VKET, bool SBRA>
-__global__ void __launch_bounds__(256, 1) fsym_block_kernel(const int2 *__restrict__ groups, int ngroups,
-                                                         int *__restrict__ qcount,
-                                                         const int *__restrict__ tstart, int LC, int K,
-                                                         int nst, Consts<N> cs,
-                                                         const double *__restrict__ bra,
-                                                         const double *__restrict__ ket,
-                                                         const double *__restrict__ C, KetMap kmap,
-                                                         double *__restrict__ H, double *__restrict__ S,
-                                                         double *__restrict__ part_b,
-                                                         double *__restrict__ part_k, int *status) {
+// The fused pass with W-warp blocks (W = 8 or 12), one per SM, persistent over
+// a queue of tile groups: group g = row block kb and ket chunks lc0 .. lc0 + W
+// - 1, one per warp.  The warps read the same 32 bras and step through their
+// terms together (fsym_tile with BSYNC), so the warps sharing a scheduler run
+// the same stretch of the long term body.  SBRA: the group's bras are staged in
+// shared memory once for all warps; SKET: each warp stages its current ket
+// record.  Shared memory (dynamic): per warp 2 PS 32 + 2 16 33 + 32 (+ the ket
+// record) doubles, then the bras.
+template <int N> __host__ __device__ constexpr int fsym_warp_smem(bool sket) {
+    return 2 * Part<N>::size * 32 + 2 * 16 * 33 + 32 + (sket ? KetLayout<N>::size : 0);
+}
+template <int N> __host__ __device__ constexpr int fsym_block_smem_bytes(int warps, bool sbra, bool sket) {
+    return (warps * fsym_warp_smem<N>(sket) + (sbra ? BraLayout<N>::size * 32 : 0)) * 8;
+}
+
+template <int N, bool VKET, bool SBRA, bool SKET, int WARPS>
+__global__ void __launch_bounds__(32 * WARPS, 1) fsym_block_kernel(const int2 *__restrict__ groups, int ngroups,
+                                                                int *__restrict__ qcount,
+                                                                const int *__restrict__ tstart, int LC, int K,
+                                                                int nst, Consts<N> cs,
+                                                                const double *__restrict__ bra,
+                                                                const double *__restrict__ ket,
+                                                                const double *__restrict__ C, KetMap kmap,
+                                                                double *__restrict__ H, double *__restrict__ S,
+                                                                double *__restrict__ part_b,
+                                                                double *__restrict__ part_k, int *status) {
     extern __shared__ double smem[];
     __shared__ int gsh;
     constexpr int PS = Part<N>::size;
-    constexpr int PER_WARP = 2 * PS * 32 + 2 * 16 * 33 + 32;
+    constexpr int PER_WARP = fsym_warp_smem<N>(SKET);
     constexpr int BS = BraLayout<N>::size;
     const int w = threadIdx.x >> 5;
     double *base = smem + w * PER_WARP;
-    double *sbra = smem + 8 * PER_WARP;  // SBRA: BS x 32 doubles after the 8 warps' areas
-    const FusedSmem sm{base, base + 2 * PS * 32, base + 2 * PS * 32 + 2 * 16 * 33};
+    double *sbra = smem + WARPS * PER_WARP;  // SBRA: BS x 32 doubles after the warps' areas
+    const FusedSmem sm{base, base + 2 * PS * 32, base + 2 * PS * 32 + 2 * 16 * 33,
+                       base + 2 * PS * 32 + 2 * 16 * 33 + 32};
     for (;;) {
         if (threadIdx.x == 0) gsh = atomicAdd(qcount, 1);
         __syncthreads();
@@ -327,21 +337,17 @@ __global__ void __launch_bounds__(256, 1) fsym_block_kernel(const int2 *__restri
         const int kb = gr.x, lc = gr.y + w;
         const int last = min(kb * 32 + 31, K - 1);
         const bool idle = lc * LC > last;  // past this block's triangle: barriers only
-        if constexpr (SBRA) {  // the group's 32 bras, once for all 8 warps
-            for (int i = threadIdx.x; i < BS * 32; i += 256) {
+        if constexpr (SBRA) {  // the group's 32 bras, once for all warps
+            for (int i = threadIdx.x; i < BS * 32; i += 32 * WARPS) {
                 const int f = i >> 5, kk = min(kb * 32 + (i & 31), K - 1);
                 sbra[i] = bra[(size_t)f * K + kk];
             }
             __syncthreads();
         }
-        fsym_tile<N, VKET, true, SBRA>(tstart[kb] + lc, make_int2(kb, lc), LC, K, nst, cs, bra, ket, C, kmap, H,
-                                       S, part_b, part_k, status, sm, idle, sbra);
+        fsym_tile<N, VKET, true, SBRA, SKET>(tstart[kb] + lc, make_int2(kb, lc), LC, K, nst, cs, bra, ket, C, kmap,
+                                             H, S, part_b, part_k, status, sm, idle, sbra);
         if constexpr (SBRA) __syncthreads();  // sbra is rewritten for the next group
     }
-}
-
-template <int N, bool SBRA> constexpr int fsym_block_smem() {
-    return (8 * (2 * Part<N>::size * 32 + 2 * 16 * 33 + 32) + (SBRA ? BraLayout<N>::size * 32 : 0)) * 8;
 }
 
 // Sum the fused-pass partials and combine out[f * K + m] = sum_H - E sum_S with
@@ -731,31 +737,38 @@ template <int N> struct Launch {
                 a.psym + (size_t)a.nstiles * 2 * Part<N>::size * 32, a.status);
         }
     }
-    template <bool SBRA> static void fsym_block(const LaunchArgs &a, cudaStream_t st) {
+    template <bool SBRA, bool SKET, int WARPS> static void fsym_block(const LaunchArgs &a, cudaStream_t st) {
         if constexpr (Part<N>::size <= 32) {
-            constexpr int smem = fsym_block_smem<N, SBRA>();
-            static bool attr = false;  // per instantiation; the size is the same on every device
-            if (!attr) {
-                cudaFuncSetAttribute(fsym_block_kernel<N, true, SBRA>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     smem);
-                attr = true;
+            constexpr int smem = fsym_block_smem_bytes<N>(WARPS, SBRA, SKET);
+            if constexpr (smem <= 232448) {
+                auto kern = fsym_block_kernel<N, true, SBRA, SKET, WARPS>;
+                static bool attr = false;  // per instantiation; the size is the same on every device
+                if (!attr) {
+                    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+                    attr = true;
+                }
+                int dev = 0, sms = 148;
+                cudaGetDevice(&dev);
+                cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+                Consts<N> cs = make_consts<N>(a.mass_h, a.ncv_h, a.efs);
+                cudaMemsetAsync(a.qcount, 0, sizeof(int), st);
+                const int grid = a.nsgroups < sms ? a.nsgroups : sms;
+                if (grid < 1) return;
+                kern<<<grid, 32 * WARPS, smem, st>>>(a.sgroups, a.nsgroups, a.qcount, a.stile_start, a.LC_s, a.K,
+                                                     a.nst, cs, a.bra, a.ket, a.C, a.kmap, a.H, a.S, a.psym,
+                                                     a.psym + (size_t)a.nstiles * 2 * Part<N>::size * 32, a.status);
             }
-            int dev = 0, sms = 148;
-            cudaGetDevice(&dev);
-            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-            Consts<N> cs = make_consts<N>(a.mass_h, a.ncv_h, a.efs);
-            cudaMemsetAsync(a.qcount, 0, sizeof(int), st);
-            const int grid = a.nsgroups < sms ? a.nsgroups : sms;
-            if (grid < 1) return;
-            fsym_block_kernel<N, true, SBRA><<<grid, 256, smem, st>>>(
-                a.sgroups, a.nsgroups, a.qcount, a.stile_start, a.LC_s, a.K, a.nst, cs, a.bra, a.ket, a.C, a.kmap,
-                a.H, a.S, a.psym, a.psym + (size_t)a.nstiles * 2 * Part<N>::size * 32, a.status);
         }
     }
     static void fsym_tiles(const LaunchArgs &a, cudaStream_t st) {
-        if ((a.minb_s == 208 || a.minb_s == 218) && a.st_end == 0 && a.sgroups && a.qcount) {
-            if (a.minb_s == 218) fsym_block<true>(a, st);
-            else fsym_block<false>(a, st);
+        if (a.minb_s >= 200 && a.st_end == 0 && a.sgroups && a.qcount) {
+            switch (a.minb_s) {  // 2xy: lockstep blocks; see fused_variant_ok
+            case 218: fsym_block<true, false, 8>(a, st); break;
+            case 228: fsym_block<true, true, 8>(a, st); break;
+            case 222: fsym_block<true, false, 12>(a, st); break;
+            case 232: fsym_block<true, true, 12>(a, st); break;
+            default: fsym_block<false, false, 8>(a, st); break;
+            }
             return;
         }
         switch (a.minb_s) {  // 100 + w: ket records read at the point of use
@@ -846,6 +859,22 @@ int launch_gsym_reduce(const LaunchArgs &a, cudaStream_t st) {
     if (a.n > 5) return -1;
     NECG_DISPATCH(a.n, gsym_reduce(a, st));
     return 0;
+}
+int fused_block_warps(int variant) { return variant == 222 || variant == 232 ? 12 : 8; }
+bool fused_variant_ok(int n, int variant) {
+    if (variant < 200) return true;
+    if (n < 1 || n > 5) return false;
+    const bool sbra = variant != 208, sket = variant == 228 || variant == 232;
+    const int warps = fused_block_warps(variant);
+    int bytes = 0;
+    switch (n) {
+    case 1: bytes = fsym_block_smem_bytes<1>(warps, sbra, sket); break;
+    case 2: bytes = fsym_block_smem_bytes<2>(warps, sbra, sket); break;
+    case 3: bytes = fsym_block_smem_bytes<3>(warps, sbra, sket); break;
+    case 4: bytes = fsym_block_smem_bytes<4>(warps, sbra, sket); break;
+    default: bytes = fsym_block_smem_bytes<5>(warps, sbra, sket); break;
+    }
+    return bytes <= 232448;
 }
 int launch_fsym(const LaunchArgs &a, cudaStream_t st) {
     if (a.n > 5) return -1;

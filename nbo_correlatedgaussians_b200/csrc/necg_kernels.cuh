@@ -45,6 +45,10 @@ int launch_gsym_reduce(const LaunchArgs &a, cudaStream_t st);
 // fused energy + symmetric gradient pass (writes H, S and split partials) and
 // its reduction (needs E in scal, i.e. after launch_rows_finalize)
 int launch_fsym(const LaunchArgs &a, cudaStream_t st);
+// lockstep-block variants of the fused pass (2xy): warps per block, and
+// whether the variant's shared memory fits for n particles
+int fused_block_warps(int variant);
+bool fused_variant_ok(int n, int variant);
 int launch_fsym_reduce(const LaunchArgs &a, cudaStream_t st);
 int launch_grad_tiles(const LaunchArgs &a, cudaStream_t st);
 int launch_grad_reduce(const LaunchArgs &a, cudaStream_t st);

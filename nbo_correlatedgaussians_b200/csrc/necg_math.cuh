@@ -143,6 +143,17 @@ struct BraSmem {
         return v;
     }
 };
+// Ket record staged in shared memory by its warp, read at the point of use
+// (a broadcast shared load, not hoisted into registers).
+struct KetSmem {
+    const double *p;
+    __device__ __forceinline__ double operator[](int i) const {
+        double v;
+        const unsigned a = (unsigned)__cvta_generic_to_shared(p + i);
+        asm volatile("ld.shared.f64 %0, [%1];" : "=d"(v) : "r"(a));
+        return v;
+    }
+};
 // Ket record read at the point of use (warp-uniform, L1 broadcast), so its
 // fields do not stay live in registers between their uses within a term.
 struct KetRefV {
