@@ -44,6 +44,8 @@ struct InstDesc {
     // fused mode
     const int *pinv, *stile_start;
     const int2 *stiles;  // the instance's fused tile list (kb, lc), on the device
+    const int2 *bgroups; // groups of 8 consecutive chunks of one row block (kb, first lc)
+    int nbgroups, pad2;
     double *psym;
     KetMap kmap;
     double cs[kConstsDoubles];
@@ -63,7 +65,7 @@ struct PlanPtrs {
     int *pref_bra;  // cumulative K            (ninst + 1)
     int *pref_ket;  // cumulative K * nst      (ninst + 1)
     int *pref_sum;  // cumulative PS * K       (ninst + 1)
-    int *pref_ft;   // cumulative fused tiles  (ninst + 1) over the instances in `order`
+    int *pref_ft;   // cumulative fused tile groups (ninst + 1) over the instances in `order`
     int *order;     // instances by decreasing tile cost (fused queue order)
     int4 *etiles;   // (inst, kb, lc, 0); fused mode: (inst, kb, lc, tile index in the instance)
     int4 *gtiles;
@@ -159,29 +161,57 @@ __global__ void __launch_bounds__(32) batch_energy_kernel(PlanPtrs p) {
     }
 }
 
-// Fused tiles of every instance: one warp per tile, pulled from one queue
-// that runs over the instances in plan order (largest tiles first) and over
-// each instance's own device tile list.  Shared memory is sized for n = 5;
-// smaller n use a prefix of it.
-__global__ void __launch_bounds__(32, 8) batch_fused_kernel(PlanPtrs p) {
-    __shared__ double sacc[2 * Part<kMaxN>::size * 32];
-    __shared__ double krow[2 * 16 * 33];
-    __shared__ double kred[32];
-    const int lane = threadIdx.x & 31;
-    const int nf = p.hdr->nf;
+// Fused pass of every instance: 8-warp blocks, one per SM, persistent over one
+// queue of tile groups that runs over the instances in plan order (largest
+// tiles first) and over each instance's groups (one 32-row block, 8 consecutive
+// ket chunks, one per warp).  The warps of a block work on the same instance and
+// bras and step through their terms together; the group's bras are staged in
+// shared memory once, each warp's current ket record too (fsym_tile with
+// BSYNC, SBRA, SKET).  Shared memory is sized for n = kMaxN.
+template <int N> __host__ __device__ constexpr int bfused_warp_smem() {
+    return 2 * Part<N>::size * 32 + 2 * 16 * 33 + 32 + KetLayout<N>::size;
+}
+constexpr int kBatchFusedSmem = (8 * bfused_warp_smem<kMaxN>() + BraLayout<kMaxN>::size * 32) * 8;
+
+template <int N>
+__device__ __forceinline__ void batch_fused_group(const InstDesc &d, int2 gr, double *smem) {
+    constexpr int PS = Part<N>::size;
+    constexpr int PER_WARP = bfused_warp_smem<N>();
+    constexpr int BS = BraLayout<N>::size;
+    const int w = threadIdx.x >> 5;
+    double *base = smem + w * PER_WARP;
+    double *sbra = smem + 8 * PER_WARP;
+    const FusedSmem sm{base, base + 2 * PS * 32, base + 2 * PS * 32 + 2 * 16 * 33,
+                       base + 2 * PS * 32 + 2 * 16 * 33 + 32};
+    const int K = d.K, kb = gr.x, lc = gr.y + w;
+    const int last = min(kb * 32 + 31, K - 1);
+    const bool idle = lc * d.lc_s > last;
+    for (int i = threadIdx.x; i < BS * 32; i += 256) {
+        const int f = i >> 5, kk = min(kb * 32 + (i & 31), K - 1);
+        sbra[i] = d.bra[(size_t)f * K + kk];
+    }
+    __syncthreads();
+    double *part_b = d.psym, *part_k = d.psym + (size_t)d.nstiles * 2 * PS * 32;
+    fsym_tile<N, true, true, true, true>(d.stile_start[kb] + lc, make_int2(kb, lc), d.lc_s, K, d.nst,
+                                         consts_of<N>(d), d.bra, d.ket, d.C, d.kmap, d.H, d.S, part_b, part_k,
+                                         d.status, sm, idle, sbra);
+    __syncthreads();  // sbra and the warps' areas are reused by the next group
+}
+
+__global__ void __launch_bounds__(256, 1) batch_fused_kernel(PlanPtrs p) {
+    extern __shared__ double smem[];
+    __shared__ int gsh;
+    const int nf = p.hdr->nf, ninst = p.hdr->ninst;
     for (;;) {
-        int t = 0;
-        if (lane == 0) t = atomicAdd(&p.hdr->qf, 1);
-        t = __shfl_sync(0xffffffffu, t, 0);
+        if (threadIdx.x == 0) gsh = atomicAdd(&p.hdr->qf, 1);
+        __syncthreads();
+        const int t = gsh;
+        __syncthreads();
         if (t >= nf) break;
-        const int j = find_inst(p.pref_ft, p.hdr->ninst, t);
+        const int j = find_inst(p.pref_ft, ninst, t);
         const InstDesc &d = p.inst[p.order[j]];
-        const int ti = t - p.pref_ft[j];  // tile index within the instance
-        const size_t PSd = (size_t)(tri(d.n) + 1 + 3 * d.n);
-        double *part_b = d.psym, *part_k = d.psym + (size_t)d.nstiles * 2 * PSd * 32;
-        BATCH_SWITCH(d.n, (fsym_tile<N, true>(ti, d.stiles[ti], d.lc_s, d.K, d.nst, consts_of<N>(d), d.bra,
-                                              d.ket, d.C, d.kmap, d.H, d.S, part_b, part_k, d.status,
-                                              FusedSmem{sacc, krow, kred})));
+        const int2 gr = d.bgroups[t - p.pref_ft[j]];
+        BATCH_SWITCH(d.n, batch_fused_group<N>(d, gr, smem));
     }
 }
 
@@ -358,7 +388,7 @@ using namespace necg;
 struct necg_batch {
     int cap_inst = 0, cap_tiles = 0;
     int device = 0, sms = 148;
-    int occ_energy = 8, occ_grad = 8, occ_fused = 8;  // resident one-warp blocks per SM (persistent kernels)
+    int occ_energy = 8, occ_grad = 8;  // resident one-warp blocks per SM (persistent kernels)
     bool fused = false;  // mode of the current plan
     char *d_plan = nullptr;  // device plan buffer
     char *h_plan = nullptr;  // pinned host staging
@@ -414,7 +444,7 @@ void launch_step(necg_batch *b, cudaStream_t st, bool fused) {
     batch_reset_kernel<<<1, 256, 0, st>>>(p);
     batch_prep_kernel<<<g * 4, 128, 0, st>>>(p);
     if (fused) {
-        batch_fused_kernel<<<g * b->occ_fused, 32, 0, st>>>(p);
+        batch_fused_kernel<<<g, 256, kBatchFusedSmem, st>>>(p);
         batch_rows_kernel<<<g * 4, 256, 0, st>>>(p);
         batch_finalize_kernel<<<g, 256, 0, st>>>(p);
         batch_fsum_kernel<<<g * 4, 256, 0, st>>>(p);
@@ -464,12 +494,12 @@ int necg_batch_create(int max_instances, int max_tiles, necg_batch **out) {
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b->occ_grad, batch_grad_kernel, 32, 0) != cudaSuccess ||
         b->occ_grad < 1)
         b->occ_grad = 8;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b->occ_fused, batch_fused_kernel, 32, 0) != cudaSuccess ||
-        b->occ_fused < 1)
-        b->occ_fused = 8;
     PlanPtrs tmp{};
     layout(b, nullptr, tmp, &b->plan_bytes);
-    cudaError_t e = cudaMalloc((void **)&b->d_plan, b->plan_bytes);
+    // the fused kernel's shared memory (one 8-warp block per SM) needs the opt-in
+    cudaError_t e = cudaFuncSetAttribute(batch_fused_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         kBatchFusedSmem);
+    if (e == cudaSuccess) e = cudaMalloc((void **)&b->d_plan, b->plan_bytes);
     if (e == cudaSuccess) e = cudaMallocHost((void **)&b->h_plan, b->plan_bytes);
     if (e == cudaSuccess) e = cudaMemset(b->d_plan, 0, b->plan_bytes);
     if (e != cudaSuccess) {
@@ -565,6 +595,8 @@ int necg_batch_plan(necg_batch *b, int count, necg_handle *const *hs, const int 
             d.psym = h->d_psym;
             d.kmap = KetMap{h->d_kcnt, h->d_ksrc, h->d_kcoef, h->kmaxnz};
             d.stiles = h->d_stiles;
+            d.bgroups = h->d_bgroups;
+            d.nbgroups = h->nbgroups;
         }
         const int ps = tri(n) + 1 + 3 * n;
         hp.pref_bra[q + 1] = hp.pref_bra[q] + K;
@@ -589,7 +621,7 @@ int necg_batch_plan(necg_batch *b, int count, necg_handle *const *hs, const int 
         std::stable_sort(hp.order, hp.order + count, [&](int a, int c) { return fcost[a] > fcost[c]; });
         hp.pref_ft[0] = 0;
         for (int j = 0; j < count; ++j) {
-            nf += hp.inst[hp.order[j]].nstiles;
+            nf += hp.inst[hp.order[j]].nbgroups;
             if (nf > 0x7fffffff) return NECG_ERR_CAPACITY;
             hp.pref_ft[j + 1] = (int)nf;
         }

@@ -59,7 +59,7 @@ void free_all(necg_handle *h) {
     void *ptrs[] = {h->d_sml, h->d_sms, h->d_scvv, h->d_bra, h->d_ket, h->d_part, h->d_H,
                     h->d_S, h->d_rows, h->d_scal, h->d_x, h->d_g, h->d_f, h->d_status,
                     h->d_tiles, h->d_pinv, h->d_kcnt, h->d_ksrc, h->d_kcoef, h->d_stiles,
-                    h->d_stile_start, h->d_psym, h->d_sgroups, h->d_qcount};
+                    h->d_stile_start, h->d_psym, h->d_sgroups, h->d_qcount, h->d_bgroups};
     for (void *p : ptrs)
         if (p) cudaFree(p);
 }
@@ -135,6 +135,19 @@ int ensure_sym_tiles(necg_handle *h, int K, cudaStream_t st, int mult) {
     CK(cudaMemcpyAsync(h->d_sgroups, groups.data(), groups.size() * sizeof(int2), cudaMemcpyHostToDevice, st));
     h->nsgroups = (int)groups.size();
     h->sgroups_w = gw;
+    std::vector<int2> bgroups;  // width 8, for the batched step
+    for (int kb = nkb - 1; kb >= 0; --kb) {
+        const int ntk = start[kb + 1] - start[kb];
+        for (int lc0 = 0; lc0 < ntk; lc0 += 8) bgroups.push_back(make_int2(kb, lc0));
+    }
+    if ((int)bgroups.size() > h->bgroups_cap) {
+        if (h->d_bgroups) cudaFree(h->d_bgroups);
+        h->d_bgroups = nullptr;
+        CK(cudaMalloc((void **)&h->d_bgroups, bgroups.size() * sizeof(int2)));
+        h->bgroups_cap = (int)bgroups.size();
+    }
+    CK(cudaMemcpyAsync(h->d_bgroups, bgroups.data(), bgroups.size() * sizeof(int2), cudaMemcpyHostToDevice, st));
+    h->nbgroups = (int)bgroups.size();
     CK(cudaMemcpyAsync(h->d_stiles, t.data(), t.size() * sizeof(int2), cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(h->d_stile_start, start.data(), start.size() * sizeof(int), cudaMemcpyHostToDevice, st));
     CK(cudaStreamSynchronize(st));

@@ -41,6 +41,8 @@ struct necg_handle {
     int2 *d_sgroups = nullptr;  // groups of 8 fused tiles of one row block (kb, first lc)
     int sgroups_cap = 0, nsgroups = 0, sgroups_w = 0;
     int *d_qcount = nullptr;    // queue head of the block-synchronised fused pass
+    int2 *d_bgroups = nullptr;  // the same groups with 8 chunks each (the batched step's blocks)
+    int bgroups_cap = 0, nbgroups = 0;
 };
 
 namespace necg {
