@@ -54,8 +54,8 @@ struct InstDesc {
 struct PlanHdr {
     int ninst, ne, ng;
     int qe, qg;  // persistent queue heads
-    int nf, qf;  // fused tile queue
-    int pad;
+    int nf, qf;  // fused queue: tile groups (lockstep kernel) or tiles (one-warp kernel)
+    int fine;    // 1: the one-warp fused kernel (few groups for the SMs)
 };
 
 // plan buffer layout: [PlanHdr][InstDesc x cap][prefix arrays][tiles]
@@ -65,7 +65,7 @@ struct PlanPtrs {
     int *pref_bra;  // cumulative K            (ninst + 1)
     int *pref_ket;  // cumulative K * nst      (ninst + 1)
     int *pref_sum;  // cumulative PS * K       (ninst + 1)
-    int *pref_ft;   // cumulative fused tile groups (ninst + 1) over the instances in `order`
+    int *pref_ft;   // cumulative fused tile groups, or tiles when fine (ninst + 1), over `order`
     int *order;     // instances by decreasing tile cost (fused queue order)
     int4 *etiles;   // (inst, kb, lc, 0); fused mode: (inst, kb, lc, tile index in the instance)
     int4 *gtiles;
@@ -158,6 +158,32 @@ __global__ void __launch_bounds__(32) batch_energy_kernel(PlanPtrs p) {
                                                            d.S, nullptr, nullptr, bad)));
             flag_inst(d.status, fl, bad);
         }
+    }
+}
+
+// Fused tiles of every instance, one warp per tile (the plan's choice when its
+// groups are too few to fill the SMs with 8-warp blocks): pulled from one queue
+// that runs over the instances in plan order and over each instance's own
+// device tile list.  Shared memory is sized for n = kMaxN.
+__global__ void __launch_bounds__(32, 8) batch_fused_warp_kernel(PlanPtrs p) {
+    __shared__ double sacc[2 * Part<kMaxN>::size * 32];
+    __shared__ double krow[2 * 16 * 33];
+    __shared__ double kred[32];
+    const int lane = threadIdx.x & 31;
+    const int nf = p.hdr->nf;
+    for (;;) {
+        int t = 0;
+        if (lane == 0) t = atomicAdd(&p.hdr->qf, 1);
+        t = __shfl_sync(0xffffffffu, t, 0);
+        if (t >= nf) break;
+        const int j = find_inst(p.pref_ft, p.hdr->ninst, t);
+        const InstDesc &d = p.inst[p.order[j]];
+        const int ti = t - p.pref_ft[j];  // tile index within the instance
+        const size_t PSd = (size_t)(tri(d.n) + 1 + 3 * d.n);
+        double *part_b = d.psym, *part_k = d.psym + (size_t)d.nstiles * 2 * PSd * 32;
+        BATCH_SWITCH(d.n, (fsym_tile<N, true>(ti, d.stiles[ti], d.lc_s, d.K, d.nst, consts_of<N>(d), d.bra,
+                                              d.ket, d.C, d.kmap, d.H, d.S, part_b, part_k, d.status,
+                                              FusedSmem{sacc, krow, kred, nullptr})));
     }
 }
 
@@ -388,15 +414,16 @@ using namespace necg;
 struct necg_batch {
     int cap_inst = 0, cap_tiles = 0;
     int device = 0, sms = 148;
-    int occ_energy = 8, occ_grad = 8;  // resident one-warp blocks per SM (persistent kernels)
+    int occ_energy = 8, occ_grad = 8, occ_fwarp = 8;  // resident one-warp blocks per SM (persistent kernels)
+    int mode = 0;  // of the current plan: 0 ordered, 1 fused lockstep, 2 fused one-warp
     bool fused = false;  // mode of the current plan
     char *d_plan = nullptr;  // device plan buffer
     char *h_plan = nullptr;  // pinned host staging
     size_t plan_bytes = 0;
     PlanPtrs ptrs{};
     std::vector<necg_handle *> active;
-    cudaGraph_t graph[2] = {};  // per mode: 0 ordered, 1 fused
-    cudaGraphExec_t exec[2] = {};
+    cudaGraph_t graph[3] = {};  // per mode
+    cudaGraphExec_t exec[3] = {};
     cudaEvent_t uploaded = nullptr;  // recorded after the last plan upload from h_plan
     int ninst = 0, ne = 0, ng = 0;
 };
@@ -438,13 +465,15 @@ void layout(necg_batch *b, char *base, PlanPtrs &p, size_t *total) {
     if (total) *total = off;
 }
 
-void launch_step(necg_batch *b, cudaStream_t st, bool fused) {
+// mode: 0 ordered, 1 fused (lockstep blocks), 2 fused (one-warp blocks)
+void launch_step(necg_batch *b, cudaStream_t st, int mode) {
     const PlanPtrs &p = b->ptrs;
     const int g = b->sms;
     batch_reset_kernel<<<1, 256, 0, st>>>(p);
     batch_prep_kernel<<<g * 4, 128, 0, st>>>(p);
-    if (fused) {
-        batch_fused_kernel<<<g, 256, kBatchFusedSmem, st>>>(p);
+    if (mode) {
+        if (mode == 2) batch_fused_warp_kernel<<<g * b->occ_fwarp, 32, 0, st>>>(p);
+        else batch_fused_kernel<<<g, 256, kBatchFusedSmem, st>>>(p);
         batch_rows_kernel<<<g * 4, 256, 0, st>>>(p);
         batch_finalize_kernel<<<g, 256, 0, st>>>(p);
         batch_fsum_kernel<<<g * 4, 256, 0, st>>>(p);
@@ -468,7 +497,7 @@ int capture(necg_batch *b, int mode) {
     BCK(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
     cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
     if (e == cudaSuccess) {
-        launch_step(b, cap, mode == 1);
+        launch_step(b, cap, mode);
         e = cudaStreamEndCapture(cap, &b->graph[mode]);
     }
     if (e == cudaSuccess) e = cudaGraphInstantiate(&b->exec[mode], b->graph[mode], 0);
@@ -496,7 +525,10 @@ int necg_batch_create(int max_instances, int max_tiles, necg_batch **out) {
         b->occ_grad = 8;
     PlanPtrs tmp{};
     layout(b, nullptr, tmp, &b->plan_bytes);
-    // the fused kernel's shared memory (one 8-warp block per SM) needs the opt-in
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b->occ_fwarp, batch_fused_warp_kernel, 32, 0) != cudaSuccess ||
+        b->occ_fwarp < 1)
+        b->occ_fwarp = 8;
+    // the lockstep fused kernel's shared memory (one 8-warp block per SM) needs the opt-in
     cudaError_t e = cudaFuncSetAttribute(batch_fused_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          kBatchFusedSmem);
     if (e == cudaSuccess) e = cudaMalloc((void **)&b->d_plan, b->plan_bytes);
@@ -516,7 +548,7 @@ int necg_batch_create(int max_instances, int max_tiles, necg_batch **out) {
 int necg_batch_destroy(necg_batch *b) {
     if (!b) return NECG_ERR_ARG;
     cudaSetDevice(b->device);
-    for (int m = 0; m < 2; ++m) {
+    for (int m = 0; m < 3; ++m) {
         if (b->exec[m]) cudaGraphExecDestroy(b->exec[m]);
         if (b->graph[m]) cudaGraphDestroy(b->graph[m]);
     }
@@ -616,12 +648,17 @@ int necg_batch_plan(necg_batch *b, int count, necg_handle *const *hs, const int 
                 gt.push_back({(double)fg * h->nst * d.lc_g, make_int4(q, kb, lc, 0)});
     }
     long long nf = 0;
-    if (fused) {  // fused queue: instances by decreasing tile cost, each over its own tile list
+    bool fine = false;
+    if (fused) {  // fused queue: instances by decreasing tile cost, each over its own groups / tiles
         for (int q = 0; q < count; ++q) hp.order[q] = q;
         std::stable_sort(hp.order, hp.order + count, [&](int a, int c) { return fcost[a] > fcost[c]; });
+        long long ng = 0;
+        for (int q = 0; q < count; ++q) ng += hp.inst[q].nbgroups;
+        fine = ng < 4LL * b->sms;  // too few groups to fill the SMs with 8-warp blocks
         hp.pref_ft[0] = 0;
         for (int j = 0; j < count; ++j) {
-            nf += hp.inst[hp.order[j]].nbgroups;
+            const InstDesc &dj = hp.inst[hp.order[j]];
+            nf += fine ? dj.nstiles : dj.nbgroups;
             if (nf > 0x7fffffff) return NECG_ERR_CAPACITY;
             hp.pref_ft[j + 1] = (int)nf;
         }
@@ -636,8 +673,10 @@ int necg_batch_plan(necg_batch *b, int count, necg_handle *const *hs, const int 
     hp.hdr->ne = fused ? 0 : (int)et.size();
     hp.hdr->ng = (int)gt.size();
     hp.hdr->nf = fused ? (int)nf : 0;
+    hp.hdr->fine = fine ? 1 : 0;
     hp.hdr->qe = hp.hdr->qg = hp.hdr->qf = 0;
     b->fused = fused;
+    b->mode = fused ? (fine ? 2 : 1) : 0;
     b->ninst = count;
     b->ne = (int)et.size();
     b->ng = (int)gt.size();
@@ -658,7 +697,7 @@ int necg_batch_plan(necg_batch *b, int count, necg_handle *const *hs, const int 
 int necg_batch_step(necg_batch *b, void *stream) {
     if (!b) return NECG_ERR_ARG;
     BCK(cudaSetDevice(b->device));
-    launch_step(b, (cudaStream_t)stream, b->fused);
+    launch_step(b, (cudaStream_t)stream, b->mode);
     return cfail(cudaGetLastError());
 }
 
@@ -666,13 +705,13 @@ int necg_batch_graph(necg_batch *b, void *stream) {
     if (!b) return NECG_ERR_ARG;
     BCK(cudaSetDevice(b->device));
     (void)stream;
-    return capture(b, b->fused ? 1 : 0);
+    return capture(b, b->mode);
 }
 
 int necg_batch_replay(necg_batch *b, void *stream) {
     if (!b) return NECG_ERR_ARG;
     BCK(cudaSetDevice(b->device));
-    const int mode = b->fused ? 1 : 0;
+    const int mode = b->mode;
     if (!b->exec[mode]) {  // the graph of this plan's mode was not captured yet
         int rc = capture(b, mode);
         if (rc) return rc;
