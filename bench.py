@@ -65,7 +65,7 @@ def parse():
     return ap.parse_args()
 
 
-DEFAULT_TILES = {"lc_e": 2, "minb_e": 16, "lc_g": 4, "minb_g": 8, "sym": 2, "lc_s": 2, "minw_s": 218}
+DEFAULT_TILES = {"lc_e": 2, "minb_e": 16, "lc_g": 4, "minb_g": 8, "sym": 2, "lc_s": 2, "minw_s": 228}
 PASS_MODE = {"ordered": 0, "symmetric": 1, "fused": 2}
 
 
@@ -312,7 +312,7 @@ def run_engine(args):
     ph_mean = ph.mean(axis=0)
     energy_flops = unordered * tf["energy"]
     if mode == 2:  # one pass over unordered pairs: H, S and both gradients
-        block = int(tiles.get("minw_s", 8)) in (208, 218)  # 8-warp lockstep blocks
+        block = int(tiles.get("minw_s", 8)) >= 200  # lockstep blocks
         kname, per_term = (f"fsym_block_kernel<{n}>" if block else f"fsym_kernel<{n}>"), "fused"
         kern_flops, kern_ms = unordered * tf["fused"], float(ph_mean[1])
         eval_flops = kern_flops
