@@ -742,13 +742,14 @@ template <int N> struct Launch {
             constexpr int smem = fsym_block_smem_bytes<N>(WARPS, SBRA, SKET);
             if constexpr (smem <= 232448) {
                 auto kern = fsym_block_kernel<N, true, SBRA, SKET, WARPS>;
-                static bool attr = false;  // per instantiation; the size is the same on every device
-                if (!attr) {
-                    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-                    attr = true;
-                }
                 int dev = 0, sms = 148;
                 cudaGetDevice(&dev);
+                // the shared-memory opt-in is per device: once per instantiation and device
+                static bool attr[64] = {};
+                if (dev < 0 || dev >= 64 || !attr[dev]) {
+                    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+                    if (dev >= 0 && dev < 64) attr[dev] = true;
+                }
                 cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
                 Consts<N> cs = make_consts<N>(a.mass_h, a.ncv_h, a.efs);
                 cudaMemsetAsync(a.qcount, 0, sizeof(int), st);
