@@ -81,7 +81,8 @@ int necg_set_variant(necg_handle *h, int minw_energy, int minw_grad);
  * set closed under inverse (each sml and sms has its inverse in the set) and
  * n <= 5; otherwise NECG_ERR_UNSUPPORTED.  lc: kets per tile (1..64); minw: 8,
  * 12 or 16 warps per SM, and for mode 2 also 108 and 112 (8 and 12 warps with
- * the ket records re-read at each use instead of held in registers) and 208
+ * the ket records re-read at each use instead of held in registers), 118 and
+ * 122 (the same with each warp's ket record staged in shared memory), 208
  * (as 108, with the 8 warps of an SM in one block stepping through their terms
  * together), 218 (as 208, with the block's bra records staged in shared
  * memory), 228 (as 218, each warp's current ket record staged too), 222 and 232

@@ -39,8 +39,9 @@ MINB = (8, 12, 16, 20)
 MINB_GRAD_EXTRA = (112, 116)  # gradient kernel with shared-memory accumulators
 LC_S = (2, 4, 8, 16)          # kets per tile of the symmetric gradient pass
 MINW_SYM = (8, 12)
-MINW_FUSED = (8, 12, 16, 108, 112, 208, 218, 228, 222, 232)
-# 100 + w: ket records re-read at each use; 2xy: lockstep blocks (208 8 warps,
+MINW_FUSED = (8, 12, 16, 108, 112, 118, 122, 208, 218, 228, 222, 232)
+# 100 + w: ket records re-read at each use (118 / 122: staged in shared memory,
+# 8 / 12 warps); 2xy: lockstep blocks (208 8 warps,
 # 218 + bras in shared memory, 228 + ket record in shared memory, 222 / 232 the
 # same with 12 warps); a variant whose shared memory does not fit for n is refused
 # by necg_set_symmetric and skipped

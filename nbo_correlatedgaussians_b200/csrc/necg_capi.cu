@@ -404,7 +404,8 @@ int necg_set_tiles(necg_handle *h, int lc_energy, int lc_grad) {
 
 int necg_set_symmetric(necg_handle *h, int mode, int lc, int minw) {
     const bool blockv = minw == 208 || minw == 218 || minw == 228 || minw == 222 || minw == 232;
-    const bool okw = minw == 8 || minw == 12 || minw == 16 || (mode == 2 && (minw == 108 || minw == 112 || blockv));
+    const bool okw = minw == 8 || minw == 12 || minw == 16 ||
+                     (mode == 2 && (minw == 108 || minw == 112 || minw == 118 || minw == 122 || blockv));
     if (!h || mode < 0 || mode > 2 || lc < 1 || lc > 64 || !okw) return NECG_ERR_ARG;
     if (blockv && !necg::fused_variant_ok(h->n, minw)) return NECG_ERR_UNSUPPORTED;  // shared memory
     if (mode && !h->sym_ok) return NECG_ERR_UNSUPPORTED;

@@ -125,6 +125,8 @@ __device__ __forceinline__ void fsym_tile(int t, int2 tl, int LC, int K, int nst
             else if constexpr (SBRA)
                 tok = term_fused<N, double>(BraSmem{sbra + lane}, KetRefV{kr}, cs, wb, wk, accH, accS, koH, koS, h,
                                             ov);
+            else if constexpr (SKET)
+                tok = term_fused<N, double>(b, KetSmem{sm.sket}, cs, wb, wk, accH, accS, koH, koS, h, ov);
             else if constexpr (VKET)
                 tok = term_fused<N, double>(b, KetRefV{kr}, cs, wb, wk, accH, accS, koH, koS, h, ov);
             else

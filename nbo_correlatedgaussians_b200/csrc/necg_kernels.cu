@@ -273,7 +273,7 @@ __global__ void __launch_bounds__(32, MINW) gsym_kernel(const int2 *__restrict__
 
 // Fused pass over unordered pairs (k >= l): one warp per tile; the body is
 // fsym_tile (necg_device.cuh), shared with the batched persistent kernel.
-template <int N, int MINW, bool VKET>
+template <int N, int MINW, bool VKET, bool SKET>
 __global__ void __launch_bounds__(32, MINW) fsym_kernel(const int2 *__restrict__ tiles, int t_begin, int t_end,
                                                    int LC, int K, int nst, Consts<N> cs,
                                                    const double *__restrict__ bra,
@@ -285,10 +285,11 @@ __global__ void __launch_bounds__(32, MINW) fsym_kernel(const int2 *__restrict__
     __shared__ double sacc[2 * Part<N>::size * 32];
     __shared__ double krow[2 * 16 * 33];
     __shared__ double kred[32];
+    __shared__ double sket[SKET ? KetLayout<N>::size : 2];
     const int t = t_begin + blockIdx.x;
     if (t >= t_end) return;
-    fsym_tile<N, VKET>(t, tiles[t], LC, K, nst, cs, bra, ket, C, kmap, H, S, part_b, part_k, status,
-                       FusedSmem{sacc, krow, kred});
+    fsym_tile<N, VKET, false, false, SKET>(t, tiles[t], LC, K, nst, cs, bra, ket, C, kmap, H, S, part_b, part_k,
+                                           status, FusedSmem{sacc, krow, kred, sket});
 }
 
 // The fused pass with W-warp blocks (W = 8 or 12), one per SM, persistent over
@@ -727,12 +728,12 @@ template <int N> struct Launch {
                                                                       a.status);
         }
     }
-    template <int MINW, bool VKET> static void fsym_v(const LaunchArgs &a, cudaStream_t st) {
+    template <int MINW, bool VKET, bool SKET = false> static void fsym_v(const LaunchArgs &a, cudaStream_t st) {
         if constexpr (Part<N>::size <= 32) {
             Consts<N> cs = make_consts<N>(a.mass_h, a.ncv_h, a.efs);
             const int t0 = a.st_end > 0 ? a.st_begin : 0, t1 = a.st_end > 0 ? a.st_end : a.nstiles;
             if (t1 <= t0) return;
-            fsym_kernel<N, MINW, VKET><<<t1 - t0, 32, 0, st>>>(
+            fsym_kernel<N, MINW, VKET, SKET><<<t1 - t0, 32, 0, st>>>(
                 a.stiles, t0, t1, a.LC_s, a.K, a.nst, cs, a.bra, a.ket, a.C, a.kmap, a.H, a.S, a.psym,
                 a.psym + (size_t)a.nstiles * 2 * Part<N>::size * 32, a.status);
         }
@@ -777,6 +778,8 @@ template <int N> struct Launch {
         case 16: fsym_v<16, false>(a, st); break;
         case 108: fsym_v<8, true>(a, st); break;
         case 112: fsym_v<12, true>(a, st); break;
+        case 118: fsym_v<8, true, true>(a, st); break;
+        case 122: fsym_v<12, true, true>(a, st); break;
         default: fsym_v<8, false>(a, st); break;
         }
     }

@@ -232,7 +232,7 @@ def test_fused_pass_matches_oracle(torch_cuda, system, K, lc):
     assert L.necg_set_symmetric(eng.h, 1, lc, 8) == _lib.NECG_OK
     f1, g1 = eng.outprod(p.x)
     fr, gr, Hr, Sr = Oracle.from_problem(p).outprod(p.x, nthreads=8, return_hs=True)
-    for minw in (8, 12, 16, 108, 112, 208, 218, 228, 222, 232):
+    for minw in (8, 12, 16, 108, 112, 118, 122, 208, 218, 228, 222, 232):
         rc = L.necg_set_symmetric(eng.h, 2, lc, minw)
         if rc == _lib.NECG_ERR_UNSUPPORTED and minw in (222, 232) and p.n == 5:
             continue  # 12 warps of n = 5 do not fit in shared memory
