@@ -98,7 +98,7 @@ __device__ __forceinline__ void fsym_tile(int t, int2 tl, int LC, int K, int nst
         }
     } koH{krow0 + (lane >> 1) * 33, !(lane & 1)}, koS{krow1 + (lane >> 1) * 33, !(lane & 1)};
     bool ok = true;
-    int flags = 0, bad = 0;
+    int flags = 0, bad = 0x7fffffff;  // smallest failing pair (row-major k K + l)
     for (int l = l0; l < l1; ++l) {
         // warp-uniform: this (l) has work (always, without BSYNC)
         const bool lok = !BSYNC || (!idle && l < K);
@@ -132,7 +132,10 @@ __device__ __forceinline__ void fsym_tile(int t, int2 tl, int LC, int K, int nst
             else
                 tok = term_fused<N, double>(b, kr, cs, wb, wk, accH, accS, koH, koS, h, ov);
             if (active) {
-                ok = tok && ok;
+                if (!tok && ok) {  // the first pair of this lane that is not positive definite
+                    ok = false;
+                    bad = min(bad, k * K + l);
+                }
                 const double w = kr[KL::w];
                 hsum += w * h;
                 ssum += w * ov;
@@ -159,7 +162,7 @@ __device__ __forceinline__ void fsym_tile(int t, int2 tl, int LC, int K, int nst
         if (BSYNC && !lok) continue;
         if (active) {
             if (!isfinite(hsum) || !isfinite(ssum)) {
-                if (!(flags & 2)) bad = k * K + l;
+                bad = min(bad, k * K + l);
                 flags |= 2;
             }
             H[(size_t)k * K + l] = hsum;
@@ -176,10 +179,7 @@ __device__ __forceinline__ void fsym_tile(int t, int2 tl, int LC, int K, int nst
 #pragma unroll
         for (int f = 0; f < 2 * PS; ++f) part_b[((size_t)t * 2 * PS + f) * 32 + lane] = sm.sacc[f * 32 + lane];
     }
-    if (!ok) {
-        flags |= 1;
-        bad = k * K + l0;
-    }
+    if (!ok) flags |= 1;
     flag_status(status, flags, bad);
     __syncwarp();
 }

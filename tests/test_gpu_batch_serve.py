@@ -142,6 +142,31 @@ def test_batch_modes_fused_and_ordered(torch_cuda):
                 res[i] = (f, g)
 
 
+@pytest.mark.parametrize("big", [False, True])
+def test_batch_failing_instance_is_isolated(torch_cuda, big):
+    """One instance with a singular A_k + A_l' in a batched step: its status is
+    NOT_PD and the other instances' results are unaffected (one-warp step for a
+    small plan; lockstep step when large instances fill the SMs)."""
+    from nbo_correlatedgaussians_b200 import _lib, synth
+    from nbo_correlatedgaussians_b200.batch import BatchEngine
+    probs = _mixed(40)
+    if big:
+        probs += [synth.make_problem("LiH", 700, 41), synth.make_problem("H2", 900, 42)]
+    bad = probs[2].copy()
+    bad.iv[3 * bad.blk:3 * bad.blk + bad.svh] = 0.0
+    allp = probs + [bad]
+    be = BatchEngine(allp, tune=False)
+    be.plan()
+    be.step(graph=True)
+    codes = be.status()
+    assert codes[-1] == _lib.NECG_ERR_NOT_PD
+    assert all(c == _lib.NECG_OK for c in codes[:-1])
+    for i, p in enumerate(probs):
+        f, g = be.results(i)
+        fo, go = Oracle.from_problem(p).outprod(p.x, nthreads=16)
+        assert abs(f - fo) < TOL_E and normwise(g, go) < TOL_G
+
+
 def test_batch_graph_replay_tracks_new_inputs(torch_cuda):
     from nbo_correlatedgaussians_b200.batch import BatchEngine
     probs = _mixed(10)

@@ -252,20 +252,24 @@ def test_fused_pass_matches_oracle(torch_cuda, system, K, lc):
         assert np.max(np.abs(Sn - Sr)) <= TOL_ELEM * max(1.0, np.max(np.abs(Sr)))
 
 
-def test_fused_pass_oldquit_and_errors(torch_cuda):
+@pytest.mark.parametrize("minw", [8, 118, 208, 228])
+def test_fused_pass_oldquit_and_errors(torch_cuda, minw):
     """The fused mode on the reference's input file, and the pair-status path
-    (a singular A_k + A_l') leaving the handle usable."""
+    (a singular A_k + A_l') leaving the handle usable, for one-warp and lockstep
+    blocks."""
     from nbo_correlatedgaussians_b200 import _lib
     d = golden("oldquit.npz")
     p = problem_from(d)
     eng = _engine(p)
-    assert eng.L.necg_set_symmetric(eng.h, 2, 4, 8) == _lib.NECG_OK
+    assert eng.L.necg_set_symmetric(eng.h, 2, 4, minw) == _lib.NECG_OK
     f, g = eng.outprod(p.x)
     assert abs(f - 4.296758204100342) < TOL_E and normwise(g, d["g"]) < TOL_G
     bad = p.copy()
     bad.iv[2 * p.blk:2 * p.blk + p.svh] = 0.0
     with pytest.raises(np.linalg.LinAlgError):
         eng.outprod(bad.x)
+    rc, pair = eng.status()
+    assert rc == _lib.NECG_ERR_NOT_PD and pair == 2 * p.K + 2  # the pair (3, 3), 1-based
     f2, g2 = eng.outprod(p.x)
     assert f2 == f and np.array_equal(g2, g)
 
