@@ -2,11 +2,14 @@
 
 Each instance (a basis of any n <= 5, nst, K) has its own ``Engine`` (handle +
 device workspace) with tile widths chosen by the autotuner for its (n, K).  A
-``BatchEngine`` plans a step over any subset of its instances: the library
-flattens all of their energy and gradient tiles into two queues ordered by
-decreasing cost, and every per-pair phase runs as one persistent launch over
-its queue.  The step is a fixed sequence of kernels with fixed grids, so it is
-captured once as a CUDA graph and replayed for every later plan.
+``BatchEngine`` plans a step over any subset of its instances: when every
+instance's symmetry set is closed under inverse, the pair work of all of them
+is one persistent launch of the fused pass over a single queue (instances by
+decreasing tile cost, each over its own tile groups; 8-warp lockstep blocks, or
+one-warp blocks when the plan is too small to fill the SMs); otherwise one
+queue of energy tiles and one of ordered gradient tiles.  The step is a fixed
+sequence of kernels with fixed grids, so each mode's step is captured once as
+a CUDA graph and replayed for every later plan.
 """
 from __future__ import annotations
 
@@ -166,6 +169,7 @@ class BatchEngine:
         return float(self.f[i].item()), self.g[i].cpu().numpy()
 
     def terms(self, active: list[int] | None = None) -> int:
-        """(k, l, P) terms one step evaluates (energy triangle + gradient square)."""
+        """(k, l, P) terms of one step counted with the reference's loop structure
+        (energy triangle + ordered gradient square), for throughput figures."""
         ids = range(len(self.problems)) if active is None else active
         return sum((p.K * (p.K + 1) // 2 + p.K * p.K) * p.nst for p in (self.problems[i] for i in ids))

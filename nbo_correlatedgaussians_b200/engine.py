@@ -10,6 +10,7 @@ Entry points mirror the reference's hot path:
   build_matrices(iv, C)     python/necg.py:36-58      -> H, S, Kinetic, Potential
   make_grad(...)            python/make_grad.py:18-90
   matel(terms), gradel(terms)  python/matel.py:28, python/gradel.py:27 (batched)
+  rrms(terms), dipole(iv, C)   python/rrms.py:21, python/necg.py:200-244
 Errors are raised like the reference raises them: a basis pair whose A_k + A_l'
 is not positive definite raises numpy.linalg.LinAlgError (np.linalg.inv does the
 same in python/matel.py:93).
