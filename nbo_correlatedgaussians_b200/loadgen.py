@@ -125,6 +125,7 @@ def served_stream(problems: list[Problem], maxfun: int, rate: float = 20.0, seed
     total = int(sum(evals))
     return {"runs": len(problems), "evals": total, "wall_s": wall, "evals_per_s": total / wall,
             "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "steps": st["steps"],
-            "mean_batch": st["mean_batch"], "gpu_step_s": st["gpu_step_s"], "plan_s": st["plan_s"],
+            "mean_batch": st["mean_batch"], "gpu_step_s": st["gpu_step_s"],
+            "gpu_idle_between_steps_s": st["gpu_idle_between_steps_s"], "plan_s": st["plan_s"],
             "arrival_rate_per_s": rate,
             "last_arrival_s": float(t_arr[-1]) if len(t_arr) else 0.0}

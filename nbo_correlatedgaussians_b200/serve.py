@@ -106,6 +106,8 @@ class Server:
         self.t_start = None
         self.evals_done = 0
         self.gpu_ms = 0.0   # device time of the batched steps (CUDA events on the server stream)
+        self.gpu_idle_ms = 0.0  # device time between consecutive steps
+        self._last_end = None
         self.plan_s = 0.0   # host time spent planning steps
 
     # ----------------------------------------------------------- lifecycle
@@ -291,6 +293,11 @@ class Server:
     def _deliver(self, reqs: list[Request], ev, bi: int, timing) -> None:
         ev.synchronize()
         self.gpu_ms += timing[0].elapsed_time(timing[1])
+        if self._last_end is not None:  # device time with no step running since the previous one
+            gap = self._last_end.elapsed_time(timing[0])
+            if gap > 0:
+                self.gpu_idle_ms += gap
+        self._last_end = timing[1]
         codes = Batch.decode(self.flags[bi][0:2 * len(reqs):2].tolist())
         now = time.perf_counter()
         for r, code in zip(reqs, codes):
@@ -318,4 +325,5 @@ class Server:
                 "mean_batch": float(np.mean(self.step_sizes)) if self.step_sizes else 0.0,
                 "p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
                 "evals_per_s": self.evals_done / wall if wall > 0 else 0.0, "wall_s": wall,
-                "gpu_step_s": self.gpu_ms * 1e-3, "plan_s": self.plan_s, "hbm_used_bytes": self.used}
+                "gpu_step_s": self.gpu_ms * 1e-3, "gpu_idle_between_steps_s": self.gpu_idle_ms * 1e-3,
+                "plan_s": self.plan_s, "hbm_used_bytes": self.used}
