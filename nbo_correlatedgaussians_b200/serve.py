@@ -62,6 +62,7 @@ class Run:
         self.x = self.g = self.f = None
         self.xh = self.gh = self.fh = None
         self.admitted = threading.Event()
+        self.admit_error: BaseException | None = None  # set when building its device state failed
         self.evals = 0
         self.closed = False
 
@@ -138,7 +139,10 @@ class Server:
 
     # ------------------------------------------------------------- clients
     def open_run(self, problem: Problem, timeout: float | None = None) -> Run:
-        """Register a run; blocks until it is admitted (memory budget and slots)."""
+        """Register a run; blocks until it is admitted (memory budget and slots).
+        If building its device state fails (the library refuses the problem,
+        or memory runs out), its reservation is released and the error is
+        raised here."""
         if problem.n > 5:
             raise ValueError("the batched path supports n <= 5")
         with self.lock:
@@ -151,6 +155,8 @@ class Server:
         self._materialise(ready)
         if not run.admitted.wait(timeout):
             raise TimeoutError("run was not admitted in time")
+        if run.admit_error is not None:
+            raise run.admit_error
         return run
 
     def close_run(self, run: Run) -> None:
@@ -203,17 +209,33 @@ class Server:
         Runs outside the server lock, so steps keep being planned meanwhile."""
         for run in runs:
             p = run.problem
-            with torch.cuda.device(self.device):
-                eng = Engine(p, device=self.device)
-                run.x = torch.from_numpy(np.ascontiguousarray(p.x)).to(self.device)
-                run.g = torch.empty_like(run.x)
-                run.f = torch.zeros(1, dtype=torch.float64, device=self.device)
-                run.xh = torch.empty(run.x.numel(), dtype=torch.float64).pin_memory()
-                run.gh = torch.empty(run.x.numel(), dtype=torch.float64).pin_memory()
-                run.fh = torch.empty(1, dtype=torch.float64).pin_memory()
-                if self.tune:
-                    tuned(eng, run.x, p.K)
-                eng.prepare_fused(p.K)
+            eng = None
+            try:
+                with torch.cuda.device(self.device):
+                    eng = Engine(p, device=self.device)
+                    run.x = torch.from_numpy(np.ascontiguousarray(p.x)).to(self.device)
+                    run.g = torch.empty_like(run.x)
+                    run.f = torch.zeros(1, dtype=torch.float64, device=self.device)
+                    run.xh = torch.empty(run.x.numel(), dtype=torch.float64).pin_memory()
+                    run.gh = torch.empty(run.x.numel(), dtype=torch.float64).pin_memory()
+                    run.fh = torch.empty(1, dtype=torch.float64).pin_memory()
+                    if self.tune:
+                        tuned(eng, run.x, p.K)
+                    eng.prepare_fused(p.K)
+            except Exception as exc:  # noqa: BLE001 -- handed to the client in open_run
+                # give back the reservation, so other runs can be admitted
+                if eng is not None:
+                    eng.close()
+                run.x = run.g = run.f = run.xh = run.gh = run.fh = None
+                run.admit_error = exc
+                with self.lock:
+                    self.pending_slots -= 1
+                    self.used -= run.bytes
+                    run.closed = True
+                    more = self._admit_locked()
+                run.admitted.set()
+                self._materialise(more)
+                continue
             with self.lock:
                 run.engine = eng
                 self.pending_slots -= 1

@@ -244,3 +244,24 @@ def test_server_admission_under_budget(torch_cuda):
     with pytest.raises(MemoryError):
         with Server(budget_bytes=1e3, max_slots=1, tune=False) as srv:
             srv.open_run(probs[0])
+
+
+def test_server_admission_failure_releases_the_reservation(torch_cuda):
+    """A run whose device state cannot be built (here a problem the library
+    rejects at creation: no symmetry terms) fails in open_run, and its budget
+    and slot go back, so the next run is admitted and served."""
+    from nbo_correlatedgaussians_b200 import synth
+    from nbo_correlatedgaussians_b200.serve import Server, workspace_estimate
+    good = synth.make_problem("He", 40, 51)
+    bad = synth.make_problem("He", 40, 52)
+    bad.sml, bad.sms, bad.scvv = bad.sml[:0], bad.sms[:0], bad.scvv[:0]
+    budget = 1.2 * max(workspace_estimate(good), 1)
+    with Server(budget_bytes=budget, max_slots=1, tune=False) as srv:
+        with pytest.raises(Exception):
+            srv.open_run(bad, timeout=60)
+        assert srv.used == 0 and srv.pending_slots == 0
+        run = srv.open_run(good, timeout=60)
+        f, g = srv.evaluate(run, good.x, timeout=60)
+        fo, go = Oracle.from_problem(good).outprod(good.x, nthreads=8)
+        assert abs(f - fo) < TOL_E and normwise(g, go) < TOL_G
+        srv.close_run(run)
