@@ -257,8 +257,10 @@ NECG_HD void symv3(const Acc &S, int off, const R (&x)[3 * N], R (&y)[3 * N]) {
 // branch F0 = sqrt(num / den).  Two reciprocal square roots give every
 // quotient and root needed:
 //   ra = a^{-1/2}:          1/a = ra^2,  fs = F0 ra
-//   q = (num den)^{-1/2}:   F0 = num q,  1/num = q^2 den
-// and F0' a^{-1/2} = (num' - F0^2 den') fs / (2 num)  (from F0^2 = num / den).
+//   q = (num den)^{-1/2}:   F0 = num q,  q^2 = 1 / (num den)
+// and, from F0^2 = num / den, F0' = F0 (num'/num - den'/den) / 2, so
+//   F0' a^{-1/2} = fs q^2 (num' den - den' num) / 2,
+// with num'/2 and den'/2 evaluated directly (halved coefficients: exact).
 #pragma nv_exec_check_disable
 template <bool GRAD, typename R>
 NECG_HD void boys(R a, R bb, R &fs, R &dfs, R &ia, R &z) {
@@ -274,11 +276,11 @@ NECG_HD void boys(R a, R bb, R &fs, R &dfs, R &ia, R &z) {
         const R F0 = num * q;
         fs = F0 * ra;
         if (GRAD) {
-            const R dN = (((5.0 * NECG_PC1 * z + 4.0 * NECG_PC2) * z + 3.0 * NECG_PC3) * z +
-                          2.0 * NECG_PC4) * z + NECG_PC5;
-            const R dD = ((((6.0 * NECG_PC6 * z + 5.0 * NECG_PC7) * z + 4.0 * NECG_PC8) * z +
-                           3.0 * NECG_PC9) * z + 2.0 * NECG_PC10) * z + NECG_PC11;
-            dfs = 0.5 * (dN - F0 * F0 * dD) * fs * (q * q * den);
+            const R dNh = (((2.5 * NECG_PC1 * z + 2.0 * NECG_PC2) * z + 1.5 * NECG_PC3) * z +
+                           NECG_PC4) * z + 0.5 * NECG_PC5;
+            const R dDh = ((((3.0 * NECG_PC6 * z + 2.5 * NECG_PC7) * z + 2.0 * NECG_PC8) * z +
+                            1.5 * NECG_PC9) * z + NECG_PC10) * z + 0.5 * NECG_PC11;
+            dfs = fs * (q * q) * (dNh * den - dDh * num);
         } else {
             dfs = R(0.0);
         }
@@ -321,8 +323,9 @@ NECG_HD void coulomb_grad(const R (&Bi)[tri(N)], const R (&T)[3 * N], const Cons
             boys<true>(a, bb, fs, dfs, ia, z);
             const double c = cs.cv[vidx(p, q)];
             rho += c * fs;
-            const R al = c * dfs * ia;
-            const R be = c * ia * (dfs * z + 0.5 * fs);
+            const R ci = c * ia;
+            const R al = ci * dfs;
+            const R be = ci * (dfs * z + 0.5 * fs);
 #pragma unroll
             for (int cc = 0; cc < 3; ++cc) Z[3 * (q - 1) + cc] += al * bv[cc];
             W[sx(q - 1, q - 1)] += be;
@@ -398,7 +401,8 @@ NECG_HD bool term_core(const BA &b, const KA &kr, const Consts<N> &cs, R (&Bi)[t
 
 // tau = 3 tr(M X) - 2 <Y, M Y>.  tr(M X) with X = A_k Bi A_l' is written through
 // the matrix with the smaller tr(M A): X = A_s - A_s Bi A_s, which keeps the
-// subtraction free of cancellation.
+// subtraction free of cancellation.  The choice differs from lane to lane, so
+// both N_s are read and one is selected (no divergent branch).
 #pragma nv_exec_check_disable
 template <int N, typename R, typename BA, typename KA>
 NECG_HD R term_tau(const BA &b, const KA &kr, const Consts<N> &cs, const R (&Bi)[tri(N)],
@@ -408,26 +412,17 @@ NECG_HD R term_tau(const BA &b, const KA &kr, const Consts<N> &cs, const R (&Bi)
     R tMX;
     {
         const R tl = kr[KL::tMA], tk = b(BL::tMA);
+        const bool use_l = tl <= tk;
         R acc = R(0.0);
-        if (tl <= tk) {
 #pragma unroll
-            for (int i = 0; i < N; ++i)
+        for (int i = 0; i < N; ++i)
 #pragma unroll
-                for (int j = 0; j <= i; ++j) {
-                    const R v = Bi[sx(i, j)] * kr[KL::Np + sx(i, j)];
-                    acc += (i == j) ? v : 2.0 * v;
-                }
-            tMX = tl - acc;
-        } else {
-#pragma unroll
-            for (int i = 0; i < N; ++i)
-#pragma unroll
-                for (int j = 0; j <= i; ++j) {
-                    const R v = Bi[sx(i, j)] * b(BL::Nk + sx(i, j));
-                    acc += (i == j) ? v : 2.0 * v;
-                }
-            tMX = tk - acc;
-        }
+            for (int j = 0; j <= i; ++j) {
+                const R nl = kr[KL::Np + sx(i, j)], nk = b(BL::Nk + sx(i, j));
+                const R v = Bi[sx(i, j)] * (use_l ? nl : nk);
+                acc += (i == j) ? v : 2.0 * v;
+            }
+        tMX = (use_l ? tl : tk) - acc;
     }
     R yMy = R(0.0);
     {
@@ -748,17 +743,17 @@ NECG_HD bool term_fused(const BA &b, const KA &kr, const Consts<N> &cs, R wb, R 
     accS.d() += 0.75 * ovb;
     koH.put(tri(N), 0.75 * Fk);
     koS.put(tri(N), 0.75 * ovk);
+    // Bi (ovb (6 N_l' + W) - 1.5 Fb B) Bi = Bi ovb (6 N_l' + W) Bi - 1.5 Fb Bi, since
+    // Bi B Bi = Bi (and the same for the ket)
     {
         R Mt[tri(N)];
         const R fb = 1.5 * Fb, fk = 1.5 * Fk, sb = 1.5 * ovb, sk = 1.5 * ovk;
 #pragma unroll
-        for (int t = 0; t < tri(N); ++t)
-            Mt[t] = ovb * (6.0 * kr[KL::Np + t] + W[t]) - fb * (b(BL::A + t) + kr[KL::Ap + t]);
-        sandwich<N>(Bi, Mt, [&](int t, R v) { accH.g(t) += v; });
+        for (int t = 0; t < tri(N); ++t) Mt[t] = ovb * (6.0 * kr[KL::Np + t] + W[t]);
+        sandwich<N>(Bi, Mt, [&](int t, R v) { accH.g(t) += v - fb * Bi[t]; });
 #pragma unroll
-        for (int t = 0; t < tri(N); ++t)
-            W[t] = ovk * (6.0 * b(BL::Nk + t) + W[t]) - fk * (b(BL::A + t) + kr[KL::Ap + t]);
-        sandwich<N>(Bi, W, [&](int t, R v) { koH.put(t, v); });
+        for (int t = 0; t < tri(N); ++t) W[t] = ovk * (6.0 * b(BL::Nk + t) + W[t]);
+        sandwich<N>(Bi, W, [&](int t, R v) { koH.put(t, v - fk * Bi[t]); });
         // S parts: Bi (-1.5 ov B) Bi = -1.5 ov Bi
 #pragma unroll
         for (int t = 0; t < tri(N); ++t) {
