@@ -62,6 +62,9 @@ def parse():
                     help="truncated-Newton runs (the first of the 256-run serving stream) for the served "
                          "latency / throughput figures; 0 skips them")
     ap.add_argument("--serve-maxfun", type=int, default=6, help="evaluations per run of that stream")
+    ap.add_argument("--serve-procs", type=int, default=-1,
+                    help="client processes for the served figures (0: clients as threads of the bench process; "
+                         "default: min(12, host cores - 2))")
     return ap.parse_args()
 
 
@@ -338,7 +341,7 @@ def run_engine(args):
         cpu = cpu_port_rate(prob, args.cpu_seconds)
     served = None
     if world == 1 and args.serve_runs > 0:
-        served = serving_figures(args.serve_runs, args.serve_maxfun)
+        served = serving_figures(args.serve_runs, args.serve_maxfun, args.serve_procs)
     out = {
         "metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
@@ -380,25 +383,34 @@ def run_engine(args):
     print(json.dumps(out), flush=True)
 
 
-def serving_figures(nruns: int, maxfun: int) -> dict:
+def serving_figures(nruns: int, maxfun: int, procs: int = -1) -> dict:
     """The served form on a prefix of the 256-run stream (n uniform over He, H2,
     LiH; K log-uniform 16-2048; seeds 4000 + j): each run is a truncated-Newton
     client making at most ``maxfun`` evaluations.  Three ways through the same
     runs: plain (one after another through the per-call host entry point),
     served with every run admitted at t = 0 (the capacity), and served with
     Poisson arrivals at 20/s (the latency figures).  Host wall clock, setup
-    (engine creation, tuning) excluded from plain and from the capacity run."""
+    (engine creation, tuning) excluded from plain and from the capacity run.  The
+    served clients run in ``procs`` client processes (their SciPy work then
+    spreads over host cores) and, for comparison, as threads of this process."""
     from nbo_correlatedgaussians_b200 import synth
     from nbo_correlatedgaussians_b200.loadgen import plain_stream, served_stream
+    if procs < 0:
+        cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+        procs = max(1, min(12, cores - 2))
     probs = synth.workload("serve256")[:nruns]
     plain = plain_stream(probs, maxfun)
-    sat = served_stream(probs, maxfun, rate=0.0)
-    poi = served_stream(probs, maxfun, rate=20.0, seed=4)
+    sat = served_stream(probs, maxfun, rate=0.0, procs=procs)
+    poi = served_stream(probs, maxfun, rate=20.0, seed=4, procs=procs)
+    sat_thr = served_stream(probs, maxfun, rate=0.0) if procs > 0 else sat
     keep = ("evals", "wall_s", "evals_per_s", "p50_ms", "p99_ms")
+    more = ("gpu_step_s", "gpu_idle_between_steps_s", "mean_batch")
     return {"workload": f"first {nruns} runs of the 256-run TN stream, maxfun {maxfun}",
+            "client_procs": procs,
             "plain": {k: plain[k] for k in keep},
-            "served_capacity": {k: sat[k] for k in keep + ("gpu_step_s", "mean_batch")},
-            "served_poisson_20_per_s": {k: poi[k] for k in keep + ("gpu_step_s", "mean_batch")},
+            "served_capacity": {k: sat[k] for k in keep + more},
+            "served_poisson_20_per_s": {k: poi[k] for k in keep + more},
+            "served_capacity_thread_clients": {k: sat_thr[k] for k in keep + more},
             "capacity_vs_plain": sat["evals_per_s"] / plain["evals_per_s"]}
 
 

@@ -47,12 +47,17 @@ typedef struct necg_handle necg_handle;
 
 /* Create a handle for one particle system and symmetry set; allocates the
  * device workspace for bases of up to K_max functions.  Host pointers.
- * Replaces the module state set up by python/read_input.py:78-157. */
+ * Replaces the module state set up by python/read_input.py:78-157.
+ * The workspace comes from the library's stream-ordered pool of the current
+ * device (freed blocks are kept there for later handles); creation waits only
+ * for the library's own stream, never for other streams' work. */
 int necg_create(int n, int nst, int K_max, double efs, const double *mass_host,
                 const double *ncv_host, const double *scvv_host, const double *sml_host,
                 const double *sms_host, necg_handle **out);
 
-/* Release a handle and its device workspace. */
+/* Release a handle and its device workspace (back to the library's pool,
+ * without synchronising the device).  No work that uses the handle may still
+ * be running: synchronise the streams that used it first. */
 int necg_destroy(necg_handle *h);
 
 /* Bytes of device workspace the handle holds. */

@@ -10,12 +10,21 @@
 //   rows  2 K_max, scal 4, x/g staging for the host-pointer entry point
 // Nothing is allocated after necg_create, so every device-pointer entry point
 // is stream-ordered and capturable in a CUDA graph once tiles for K exist.
+//
+// Handle memory comes from one stream-ordered pool per device (cudaMemPool_t,
+// blocks kept for reuse), allocated and freed on the library's own
+// non-blocking stream of that device, or on the caller's stream when an
+// evaluation grows a buffer.  Unlike cudaMalloc / cudaFree, creating and
+// destroying a handle then never waits for work that other streams have in
+// flight, so a server can admit and retire runs while its steps keep running.
 #include <cuda_runtime.h>
 #include <math.h>
+#include <stdint.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
 
+#include <mutex>
 #include <vector>
 
 #include "necg_handle.h"
@@ -37,14 +46,66 @@ int cuda_fail(cudaError_t e) {
         if (_e != cudaSuccess) return cuda_fail(_e); \
     } while (0)
 
+// The per-device pool and stream, made on first use with that device current.
+struct DevicePool {
+    std::once_flag once;
+    cudaMemPool_t pool = nullptr;
+    cudaStream_t stream = nullptr;
+    cudaError_t err = cudaSuccess;
+};
+DevicePool g_pools[64];
+
+cudaError_t device_pool(int dev, cudaMemPool_t *pool, cudaStream_t *stream) {
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    DevicePool &d = g_pools[dev];
+    std::call_once(d.once, [&] {
+        cudaMemPoolProps props;
+        memset(&props, 0, sizeof(props));
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        d.err = cudaMemPoolCreate(&d.pool, &props);
+        if (d.err == cudaSuccess) {
+            uint64_t keep = UINT64_MAX;  // freed blocks stay in the pool for the next handle
+            d.err = cudaMemPoolSetAttribute(d.pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        }
+        if (d.err == cudaSuccess) d.err = cudaStreamCreateWithFlags(&d.stream, cudaStreamNonBlocking);
+    });
+    *pool = d.pool;
+    *stream = d.stream;
+    return d.err;
+}
+
+// Stream-ordered allocation from the handle's device pool on stream st (the
+// library stream when st is null).
+template <typename T> cudaError_t pool_alloc(necg_handle *h, T **p, size_t bytes, cudaStream_t st = nullptr) {
+    cudaMemPool_t pool;
+    cudaStream_t ls;
+    cudaError_t e = device_pool(h->device, &pool, &ls);
+    if (e == cudaSuccess) e = cudaMallocFromPoolAsync((void **)p, bytes, pool, st ? st : ls);
+    if (e != cudaSuccess) *p = nullptr;
+    return e;
+}
+
+void pool_free(necg_handle *h, void *p, cudaStream_t st = nullptr) {
+    if (!p) return;
+    cudaMemPool_t pool;
+    cudaStream_t ls;
+    if (device_pool(h->device, &pool, &ls) == cudaSuccess) cudaFreeAsync(p, st ? st : ls);
+}
+
+cudaStream_t lib_stream(necg_handle *h) {
+    cudaMemPool_t pool;
+    cudaStream_t ls = nullptr;
+    device_pool(h->device, &pool, &ls);
+    return ls;
+}
+
 template <typename T> int dalloc(necg_handle *h, T **p, size_t count) {
     size_t bytes = count * sizeof(T);
     if (bytes == 0) bytes = 16;
-    cudaError_t e = cudaMalloc((void **)p, bytes);
-    if (e != cudaSuccess) {
-        *p = nullptr;
-        return cuda_fail(e);
-    }
+    cudaError_t e = pool_alloc(h, p, bytes);
+    if (e != cudaSuccess) return cuda_fail(e);
     h->ws_bytes += (long long)bytes;
     return NECG_OK;
 }
@@ -60,8 +121,7 @@ void free_all(necg_handle *h) {
                     h->d_S, h->d_rows, h->d_scal, h->d_x, h->d_g, h->d_f, h->d_status,
                     h->d_tiles, h->d_pinv, h->d_kcnt, h->d_ksrc, h->d_kcoef, h->d_stiles,
                     h->d_stile_start, h->d_psym, h->d_sgroups, h->d_qcount, h->d_bgroups};
-    for (void *p : ptrs)
-        if (p) cudaFree(p);
+    for (void *p : ptrs) pool_free(h, p);
 }
 
 // Energy tiles over the lower triangle: (kb, lc) with lc * LC <= kb * 32 + 31.
@@ -74,9 +134,9 @@ int ensure_tiles(necg_handle *h, int K, cudaStream_t st) {
         for (int lc = 0; lc * h->lc_e <= kmax && lc * h->lc_e < K; ++lc) t.push_back(make_int2(kb, lc));
     }
     if ((int)t.size() > h->tiles_cap) {
-        if (h->d_tiles) cudaFree(h->d_tiles);
+        pool_free(h, h->d_tiles, st);
         h->d_tiles = nullptr;
-        CK(cudaMalloc((void **)&h->d_tiles, t.size() * sizeof(int2)));
+        CK(pool_alloc(h, &h->d_tiles, t.size() * sizeof(int2), st));
         h->tiles_cap = (int)t.size();
     }
     CK(cudaMemcpyAsync(h->d_tiles, t.data(), t.size() * sizeof(int2), cudaMemcpyHostToDevice, st));
@@ -106,17 +166,17 @@ int ensure_sym_tiles(necg_handle *h, int K, cudaStream_t st, int mult) {
     }
     start.push_back((int)t.size());
     if ((int)t.size() > h->stiles_cap) {
-        if (h->d_stiles) cudaFree(h->d_stiles);
+        pool_free(h, h->d_stiles, st);
         h->d_stiles = nullptr;
-        CK(cudaMalloc((void **)&h->d_stiles, t.size() * sizeof(int2)));
+        CK(pool_alloc(h, &h->d_stiles, t.size() * sizeof(int2), st));
         h->stiles_cap = (int)t.size();
     }
-    if (!h->d_stile_start) CK(cudaMalloc((void **)&h->d_stile_start, ((h->K_max + 31) / 32 + 2) * sizeof(int)));
+    if (!h->d_stile_start) CK(pool_alloc(h, &h->d_stile_start, ((h->K_max + 31) / 32 + 2) * sizeof(int), st));
     const size_t need = t.size() * (size_t)PS * (32 + LC) * mult;
     if (need > h->psym_cap) {
-        if (h->d_psym) cudaFree(h->d_psym);
+        pool_free(h, h->d_psym, st);
         h->d_psym = nullptr;
-        CK(cudaMalloc((void **)&h->d_psym, need * sizeof(double)));
+        CK(pool_alloc(h, &h->d_psym, need * sizeof(double), st));
         h->ws_bytes += (long long)((need - h->psym_cap) * sizeof(double));
         h->psym_cap = need;
     }
@@ -126,12 +186,12 @@ int ensure_sym_tiles(necg_handle *h, int K, cudaStream_t st, int mult) {
         for (int lc0 = 0; lc0 < ntk; lc0 += gw) groups.push_back(make_int2(kb, lc0));
     }
     if ((int)groups.size() > h->sgroups_cap) {
-        if (h->d_sgroups) cudaFree(h->d_sgroups);
+        pool_free(h, h->d_sgroups, st);
         h->d_sgroups = nullptr;
-        CK(cudaMalloc((void **)&h->d_sgroups, groups.size() * sizeof(int2)));
+        CK(pool_alloc(h, &h->d_sgroups, groups.size() * sizeof(int2), st));
         h->sgroups_cap = (int)groups.size();
     }
-    if (!h->d_qcount) CK(cudaMalloc((void **)&h->d_qcount, sizeof(int)));
+    if (!h->d_qcount) CK(pool_alloc(h, &h->d_qcount, sizeof(int), st));
     CK(cudaMemcpyAsync(h->d_sgroups, groups.data(), groups.size() * sizeof(int2), cudaMemcpyHostToDevice, st));
     h->nsgroups = (int)groups.size();
     h->sgroups_w = gw;
@@ -141,9 +201,9 @@ int ensure_sym_tiles(necg_handle *h, int K, cudaStream_t st, int mult) {
         for (int lc0 = 0; lc0 < ntk; lc0 += 8) bgroups.push_back(make_int2(kb, lc0));
     }
     if ((int)bgroups.size() > h->bgroups_cap) {
-        if (h->d_bgroups) cudaFree(h->d_bgroups);
+        pool_free(h, h->d_bgroups, st);
         h->d_bgroups = nullptr;
-        CK(cudaMalloc((void **)&h->d_bgroups, bgroups.size() * sizeof(int2)));
+        CK(pool_alloc(h, &h->d_bgroups, bgroups.size() * sizeof(int2), st));
         h->bgroups_cap = (int)bgroups.size();
     }
     CK(cudaMemcpyAsync(h->d_bgroups, bgroups.data(), bgroups.size() * sizeof(int2), cudaMemcpyHostToDevice, st));
@@ -231,10 +291,12 @@ int setup_symmetric(necg_handle *h) {
     if (!rc) rc = dalloc(h, &h->d_ksrc, src.size());
     if (!rc) rc = dalloc(h, &h->d_kcoef, coef.size());
     if (rc) return rc;
-    CK(cudaMemcpy(h->d_pinv, pinv.data(), nst * sizeof(int), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(h->d_kcnt, cnt.data(), cnt.size() * sizeof(int), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(h->d_ksrc, src.data(), src.size() * sizeof(int), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(h->d_kcoef, coef.data(), coef.size() * sizeof(double), cudaMemcpyHostToDevice));
+    cudaStream_t ls = lib_stream(h);
+    CK(cudaMemcpyAsync(h->d_pinv, pinv.data(), nst * sizeof(int), cudaMemcpyHostToDevice, ls));
+    CK(cudaMemcpyAsync(h->d_kcnt, cnt.data(), cnt.size() * sizeof(int), cudaMemcpyHostToDevice, ls));
+    CK(cudaMemcpyAsync(h->d_ksrc, src.data(), src.size() * sizeof(int), cudaMemcpyHostToDevice, ls));
+    CK(cudaMemcpyAsync(h->d_kcoef, coef.data(), coef.size() * sizeof(double), cudaMemcpyHostToDevice, ls));
+    CK(cudaStreamSynchronize(ls));  // the host vectors above end with this scope
     h->kmaxnz = maxnz;
     h->sym_ok = true;
     h->grad_mode = 1;
@@ -370,11 +432,14 @@ int necg_create(int n, int nst, int K_max, double efs, const double *mass_host,
     if (!rc) rc = dalloc(h, &h->d_g, K * blk + K);
     if (!rc) rc = dalloc(h, &h->d_f, (size_t)2);
     if (!rc) rc = dalloc(h, &h->d_status, (size_t)4);
-    if (!rc) rc = cuda_fail(cudaMemcpy(h->d_sml, h->sml.data(), h->sml.size() * 8, cudaMemcpyHostToDevice));
-    if (!rc) rc = cuda_fail(cudaMemcpy(h->d_sms, h->sms.data(), h->sms.size() * 8, cudaMemcpyHostToDevice));
-    if (!rc) rc = cuda_fail(cudaMemcpy(h->d_scvv, h->scvv.data(), h->scvv.size() * 8, cudaMemcpyHostToDevice));
-    if (!rc) rc = cuda_fail(cudaMemset(h->d_status, 0, 16));
+    cudaStream_t ls = rc ? nullptr : lib_stream(h);
+    if (!rc) rc = cuda_fail(cudaMemcpyAsync(h->d_sml, h->sml.data(), h->sml.size() * 8, cudaMemcpyHostToDevice, ls));
+    if (!rc) rc = cuda_fail(cudaMemcpyAsync(h->d_sms, h->sms.data(), h->sms.size() * 8, cudaMemcpyHostToDevice, ls));
+    if (!rc) rc = cuda_fail(cudaMemcpyAsync(h->d_scvv, h->scvv.data(), h->scvv.size() * 8, cudaMemcpyHostToDevice, ls));
+    if (!rc) rc = cuda_fail(cudaMemsetAsync(h->d_status, 0, 16, ls));
     if (!rc) rc = setup_symmetric(h);
+    // the workspace is allocated in the library stream's order: make it usable on every stream
+    if (!rc) rc = cuda_fail(cudaStreamSynchronize(ls));
     if (rc) {
         free_all(h);
         delete h;

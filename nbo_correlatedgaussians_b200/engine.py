@@ -65,8 +65,14 @@ class Engine:
         self._g = None
 
     # ------------------------------------------------------------------ util
-    def close(self) -> None:
+    def close(self, sync: bool = True) -> None:
+        """Release the handle.  necg_destroy returns the workspace to the
+        library's device pool without waiting for the GPU, so no work that uses
+        it may still be running: by default the device is synchronised first;
+        a caller that knows its work has completed passes sync=False."""
         if getattr(self, "h", None):
+            if sync:
+                torch.cuda.synchronize(self.device)
             self.L.necg_destroy(self.h)
             self.h = None
 

@@ -8,36 +8,29 @@ Two ways to serve the same runs:
                  point (Engine.outprod: copy x in, one evaluation, copy f, g out)
   served_stream  the runs as concurrent clients of a continuous-batching
                  ``Server``; runs arrive as a Poisson process (or all at t=0,
-                 which measures the server's capacity)
+                 which measures the server's capacity).  The clients are
+                 threads of this process, or (procs > 0) threads of that many
+                 client processes connected through a ``serve.Endpoint``, so
+                 that their optimiser work runs on several host cores
 Results of a run do not depend on which other runs share a step (the batched
 tiles and reductions are the same alone and in any mix), so both ways make the
 same evaluations and the evaluation counts match.
 """
 from __future__ import annotations
 
+import multiprocessing as mp
 import threading
 import time
 
 import numpy as np
-from scipy.optimize import minimize
 
 from .autotune import tuned
+from .clients import client_worker, tn_run
 from .engine import Engine
 from .problem import Problem
-from .serve import Server
+from .serve import Endpoint, Server
 
-
-def tn_run(evaluate, x0: np.ndarray, maxfun: int) -> int:
-    """One truncated-Newton run of at most ``maxfun`` evaluations; returns the
-    number of evaluations made."""
-    count = [0]
-
-    def fun(x):
-        count[0] += 1
-        return evaluate(x)
-
-    minimize(fun, x0, method="TNC", jac=True, options={"maxfun": int(maxfun)})
-    return count[0]
+__all__ = ["tn_run", "arrival_times", "plain_stream", "served_stream"]
 
 
 def arrival_times(n: int, rate: float, seed: int) -> np.ndarray:
@@ -75,10 +68,14 @@ def plain_stream(problems: list[Problem], maxfun: int, tune: bool = True) -> dic
 
 
 def served_stream(problems: list[Problem], maxfun: int, rate: float = 20.0, seed: int = 4,
-                  budget_bytes: float = 120e9, max_slots: int = 256, tune: bool = True) -> dict:
+                  budget_bytes: float = 120e9, max_slots: int = 256, tune: bool = True,
+                  procs: int = 0) -> dict:
     """The runs as concurrent clients of one Server: run j opens at its
     arrival time (admission waits for HBM budget and a slot), makes its TN
-    evaluations back to back, and closes."""
+    evaluations back to back, and closes.  procs > 0: the clients are spread
+    over that many client processes."""
+    if procs > 0:
+        return _served_stream_procs(problems, maxfun, rate, seed, budget_bytes, max_slots, tune, procs)
     t_arr = arrival_times(len(problems), rate, seed)
     evals = [0] * len(problems)
     errors = []
@@ -128,4 +125,58 @@ def served_stream(problems: list[Problem], maxfun: int, rate: float = 20.0, seed
             "mean_batch": st["mean_batch"], "gpu_step_s": st["gpu_step_s"],
             "gpu_idle_between_steps_s": st["gpu_idle_between_steps_s"], "plan_s": st["plan_s"],
             "arrival_rate_per_s": rate,
+            "last_arrival_s": float(t_arr[-1]) if len(t_arr) else 0.0}
+
+
+def _served_stream_procs(problems, maxfun, rate, seed, budget_bytes, max_slots, tune, procs) -> dict:
+    from .serve import workspace_estimate
+    t_arr = arrival_times(len(problems), rate, seed)
+    saturate = rate <= 0 and len(problems) <= max_slots and \
+        sum(workspace_estimate(p) for p in problems) <= budget_bytes
+    ctx = mp.get_context("spawn")  # client processes never touch CUDA
+    gate = ctx.Barrier(len(problems) + 1) if saturate else None
+    go = ctx.Event()
+    t0_epoch = ctx.Value("d", 0.0)
+    out_q = ctx.Queue()
+    procs = max(1, min(int(procs), len(problems)))
+    ready = ctx.Barrier(procs + 1)
+    with Server(budget_bytes=budget_bytes, max_slots=max_slots, tune=tune) as srv:
+        ep = Endpoint(srv)
+        try:
+            jobs = [[] for _ in range(procs)]
+            for j, p in enumerate(problems):
+                jobs[j % procs].append((j, p, float(t_arr[j])))
+            workers = [ctx.Process(target=client_worker, args=(ep.address, ep.authkey, jobs[w], maxfun, ready, gate,
+                                                               go, t0_epoch, out_q), daemon=True)
+                       for w in range(procs)]
+            for w in workers:
+                w.start()
+            ready.wait(timeout=300)  # every client process has started
+            if gate is not None:
+                try:
+                    gate.wait()  # every run admitted: time the capacity from here
+                except threading.BrokenBarrierError:
+                    pass
+                t0 = time.time()
+            else:
+                t0 = time.time()
+                t0_epoch.value = t0
+                go.set()
+            srv.t_start = time.perf_counter() + (t0 - time.time())
+            results = [out_q.get() for _ in workers]
+            for w in workers:
+                w.join()
+            st = srv.stats()
+        finally:
+            ep.close()
+    errors = [e for r in results for e in r["errors"]]
+    if errors:
+        raise RuntimeError(f"{len(errors)} runs failed, first: {errors[0]}")
+    evals = sum(n for r in results for n in r["evals"].values())
+    wall = max(t for r in results for t in r["t_done"].values()) - t0
+    return {"runs": len(problems), "evals": int(evals), "wall_s": wall, "evals_per_s": evals / wall,
+            "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "steps": st["steps"],
+            "mean_batch": st["mean_batch"], "gpu_step_s": st["gpu_step_s"],
+            "gpu_idle_between_steps_s": st["gpu_idle_between_steps_s"], "plan_s": st["plan_s"],
+            "arrival_rate_per_s": rate, "client_procs": procs,
             "last_arrival_s": float(t_arr[-1]) if len(t_arr) else 0.0}

@@ -17,12 +17,19 @@ the reference's optimiser, python/necg.py:159-171 and source/tn.f).  The server:
   and the GPU does not wait for the host to deliver results.
 * reports per-request latency (submit to result) and throughput.
 
+Clients may be threads of this process (``open_run`` / ``evaluate``) or other
+processes connected through an ``Endpoint`` (``clients.RemoteRun``); the
+requests of both kinds go into the same steps.
+
 Because every run's tiles and reductions are the same in any batch, a run's
 results do not depend on which other runs share its steps.
 """
 from __future__ import annotations
 
 import collections
+import pickle
+import secrets
+import struct
 import threading
 import time
 
@@ -30,6 +37,7 @@ import numpy as np
 import torch
 
 from . import _lib
+from .clients import OP_CLOSE, OP_EVAL, OP_OPEN, REPLY_OK, encode_error
 from .autotune import tuned
 from .batch import Batch
 from .engine import Engine
@@ -65,6 +73,7 @@ class Run:
         self.admit_error: BaseException | None = None  # set when building its device state failed
         self.evals = 0
         self.closed = False
+        self.inflight = 0  # requests of this run in launched, undelivered steps
 
 
 class Request:
@@ -100,6 +109,7 @@ class Server:
         self.latencies: list[float] = []
         self.steps = 0
         self.step_sizes: list[int] = []
+        self.step_log: list[tuple] = []  # per step: host time delivered, requests, device ms, idle ms before it
         self._stop = False
         self._thread = None
         self.batches = None
@@ -160,18 +170,31 @@ class Server:
         return run
 
     def close_run(self, run: Run) -> None:
+        """Close a run: its requests not yet in a step fail, and its device
+        state is freed once the steps holding its requests are delivered.  The
+        server keeps planning and launching steps meanwhile (the wait and the
+        free run outside the server lock)."""
         with self.lock:
             if run.closed:
                 return
             run.closed = True
             self.runs.pop(run.id, None)
-            if run.engine is not None:
-                self.used -= run.bytes
-                # free after in-flight steps that may still reference this run
-                eng = run.engine
-                run.engine = None
-                self.stream.synchronize()
-                eng.close()
+            keep: collections.deque[Request] = collections.deque()
+            for r in self.pending:
+                if r.run is run:
+                    r.error = RuntimeError("run was closed before this request was served")
+                    r.done.set()
+                else:
+                    keep.append(r)
+            self.pending = keep
+            while run.inflight > 0:
+                self.lock.wait()
+            eng, run.engine = run.engine, None
+        if eng is None:
+            return
+        eng.close(sync=False)  # its steps are delivered, so none of its work is running
+        with self.lock:
+            self.used -= run.bytes
             ready = self._admit_locked()
         self._materialise(ready)
 
@@ -181,6 +204,8 @@ class Server:
             raise RuntimeError("run is not admitted or already closed")
         req = Request(run, np.ascontiguousarray(x, dtype=np.float64))
         with self.lock:
+            if run.closed:
+                raise RuntimeError("run is closed")
             self.pending.append(req)
             self.lock.notify_all()
         if not req.done.wait(timeout):
@@ -269,6 +294,7 @@ class Server:
                             rest.append(r)
                         else:
                             seen.add(r.run.id)
+                            r.run.inflight += 1
                             reqs.append(r)
                     self.pending = rest
                     bi = self.free_batches.popleft()
@@ -314,12 +340,15 @@ class Server:
 
     def _deliver(self, reqs: list[Request], ev, bi: int, timing) -> None:
         ev.synchronize()
-        self.gpu_ms += timing[0].elapsed_time(timing[1])
+        dev_ms = timing[0].elapsed_time(timing[1])
+        self.gpu_ms += dev_ms
+        gap = 0.0
         if self._last_end is not None:  # device time with no step running since the previous one
-            gap = self._last_end.elapsed_time(timing[0])
-            if gap > 0:
-                self.gpu_idle_ms += gap
+            gap = max(0.0, self._last_end.elapsed_time(timing[0]))
+            self.gpu_idle_ms += gap
         self._last_end = timing[1]
+        if len(self.step_log) < 100000:
+            self.step_log.append((time.perf_counter(), len(reqs), dev_ms, gap))
         codes = Batch.decode(self.flags[bi][0:2 * len(reqs):2].tolist())
         now = time.perf_counter()
         for r, code in zip(reqs, codes):
@@ -336,6 +365,8 @@ class Server:
             self.evals_done += 1
             r.done.set()
         with self.lock:
+            for r in reqs:
+                r.run.inflight -= 1
             self.free_batches.append(bi)
             self.lock.notify_all()
 
@@ -349,3 +380,70 @@ class Server:
                 "evals_per_s": self.evals_done / wall if wall > 0 else 0.0, "wall_s": wall,
                 "gpu_step_s": self.gpu_ms * 1e-3, "gpu_idle_between_steps_s": self.gpu_idle_ms * 1e-3,
                 "plan_s": self.plan_s, "hbm_used_bytes": self.used}
+
+
+class Endpoint:
+    """Front end of a ``Server`` for clients in other processes
+    (``clients.RemoteRun``): a listener on 127.0.0.1 (a free port, an
+    authentication key) and one handler thread per connection, each connection
+    carrying one run.  A handler turns the connection's requests into
+    ``open_run`` / ``evaluate`` / ``close_run`` calls, so remote requests join
+    the same batched steps as in-process ones; a dropped connection closes its
+    run."""
+
+    def __init__(self, srv: Server, authkey: bytes | None = None):
+        from multiprocessing.connection import Listener
+        self.srv = srv
+        self.authkey = authkey if authkey is not None else secrets.token_bytes(16)
+        self.listener = Listener(("127.0.0.1", 0), backlog=1024, authkey=self.authkey)  # runs connect together
+        self.address = self.listener.address
+        self._closed = False
+        self._thread = threading.Thread(target=self._accept, name="necg-endpoint", daemon=True)
+        self._thread.start()
+
+    def _accept(self) -> None:
+        while not self._closed:
+            try:
+                conn = self.listener.accept()
+            except Exception:  # noqa: BLE001 -- listener closed, or a client failed the handshake
+                continue
+            threading.Thread(target=self._serve, args=(conn,), name="necg-endpoint-run", daemon=True).start()
+
+    def _serve(self, conn) -> None:
+        run = None
+        try:
+            while True:
+                try:
+                    msg = conn.recv_bytes()
+                except (EOFError, OSError):
+                    return
+                op = msg[:1]
+                try:
+                    if op == OP_EVAL:
+                        if run is None:
+                            raise RuntimeError("no run is open on this connection")
+                        f, g = self.srv.evaluate(run, np.frombuffer(msg, dtype=np.float64, offset=1))
+                        conn.send_bytes(REPLY_OK + struct.pack("<d", f) + g.tobytes())
+                    elif op == OP_OPEN:
+                        if run is not None:
+                            raise RuntimeError("a run is already open on this connection")
+                        problem, timeout = pickle.loads(msg[1:])
+                        run = self.srv.open_run(problem, timeout=timeout)
+                        conn.send_bytes(REPLY_OK + struct.pack("<q", run.id))
+                    elif op == OP_CLOSE:
+                        if run is not None:
+                            self.srv.close_run(run)
+                            run = None
+                        conn.send_bytes(REPLY_OK)
+                    else:
+                        raise ValueError(f"unknown request {op!r}")
+                except Exception as exc:  # noqa: BLE001 -- returned to the client
+                    conn.send_bytes(encode_error(exc))
+        finally:
+            if run is not None:
+                self.srv.close_run(run)
+            conn.close()
+
+    def close(self) -> None:
+        self._closed = True
+        self.listener.close()

@@ -265,3 +265,33 @@ def test_server_admission_failure_releases_the_reservation(torch_cuda):
         fo, go = Oracle.from_problem(good).outprod(good.x, nthreads=8)
         assert abs(f - fo) < TOL_E and normwise(g, go) < TOL_G
         srv.close_run(run)
+
+
+def test_server_endpoint_remote_run(torch_cuda):
+    """A run driven through the cross-process front end (serve.Endpoint,
+    clients.RemoteRun) gets the same f and g as an in-process run of the same
+    server, and a failing evaluation comes back as LinAlgError."""
+    from nbo_correlatedgaussians_b200 import synth
+    from nbo_correlatedgaussians_b200.clients import RemoteRun
+    from nbo_correlatedgaussians_b200.serve import Endpoint, Server
+    p = synth.make_problem("LiH", 24, 61)
+    with Server(max_slots=4, tune=False) as srv:
+        ep = Endpoint(srv)
+        try:
+            rr = RemoteRun(ep.address, ep.authkey, p, timeout=60)
+            f, g = rr.evaluate(p.x)
+            local = srv.open_run(p, timeout=60)
+            fl, gl = srv.evaluate(local, p.x, timeout=60)
+            assert f == fl and np.array_equal(g, gl)
+            fo, go = Oracle.from_problem(p).outprod(p.x, nthreads=8)
+            assert abs(f - fo) < TOL_E and normwise(g, go) < TOL_G
+            bad = p.x.copy()
+            bad[2 * p.blk:2 * p.blk + p.svh] = 0.0
+            with pytest.raises(np.linalg.LinAlgError):
+                rr.evaluate(bad)
+            f2, _ = rr.evaluate(p.x)
+            assert f2 == f
+            rr.close()
+            srv.close_run(local)
+        finally:
+            ep.close()
