@@ -58,7 +58,7 @@ def parse():
                     help="force the pair pass (auto: the autotuner's choice)")
     ap.add_argument("--no-tune", action="store_true",
                     help="skip the autotuner and use the default tiles (for short profiling runs)")
-    ap.add_argument("--serve-runs", type=int, default=64,
+    ap.add_argument("--serve-runs", type=int, default=256,
                     help="truncated-Newton runs (the first of the 256-run serving stream) for the served "
                          "latency / throughput figures; 0 skips them")
     ap.add_argument("--serve-maxfun", type=int, default=6, help="evaluations per run of that stream")
