@@ -19,6 +19,7 @@ same evaluations and the evaluation counts match.
 from __future__ import annotations
 
 import multiprocessing as mp
+import queue
 import threading
 import time
 
@@ -154,16 +155,23 @@ def _served_stream_procs(problems, maxfun, rate, seed, budget_bytes, max_slots, 
             ready.wait(timeout=300)  # every client process has started
             if gate is not None:
                 try:
-                    gate.wait()  # every run admitted: time the capacity from here
+                    gate.wait(timeout=1800)  # every run admitted: time the capacity from here
                 except threading.BrokenBarrierError:
-                    pass
+                    pass  # a run failed to open; its client reports it
                 t0 = time.time()
             else:
                 t0 = time.time()
                 t0_epoch.value = t0
                 go.set()
             srv.t_start = time.perf_counter() + (t0 - time.time())
-            results = [out_q.get() for _ in workers]
+            results = []
+            while len(results) < len(workers):
+                try:
+                    results.append(out_q.get(timeout=1.0))
+                except queue.Empty:
+                    dead = [w.exitcode for w in workers if w.exitcode not in (None, 0)]
+                    if dead:
+                        raise RuntimeError(f"a client process exited with code {dead[0]}") from None
             for w in workers:
                 w.join()
             st = srv.stats()

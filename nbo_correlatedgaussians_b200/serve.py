@@ -206,6 +206,8 @@ class Server:
         with self.lock:
             if run.closed:
                 raise RuntimeError("run is closed")
+            if self._stop:
+                raise RuntimeError("server is stopped")
             self.pending.append(req)
             self.lock.notify_all()
         if not req.done.wait(timeout):
