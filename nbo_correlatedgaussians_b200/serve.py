@@ -202,7 +202,10 @@ class Server:
         """E and gradient at x = [iv, C] for this run (blocking)."""
         if run.engine is None:
             raise RuntimeError("run is not admitted or already closed")
-        req = Request(run, np.ascontiguousarray(x, dtype=np.float64))
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        if x.ndim != 1 or x.size != run.x.numel():
+            raise ValueError(f"x has shape {x.shape}, expected ({run.x.numel()},)")
+        req = Request(run, x)
         with self.lock:
             if run.closed:
                 raise RuntimeError("run is closed")

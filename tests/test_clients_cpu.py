@@ -89,6 +89,19 @@ def test_admission_error_and_wrong_key(endpoint):
     assert not srv.open
 
 
+def test_malformed_requests(endpoint):
+    srv, ep = endpoint
+    run = RemoteRun(ep.address, ep.authkey, synth.make_problem("He", 8, 3))
+    with pytest.raises(ValueError):
+        run._call(b"Z")  # unknown request
+    with pytest.raises(RuntimeError):
+        run._call(b"O" + __import__("pickle").dumps((synth.make_problem("He", 8, 3), None)))  # second open
+    f, _ = run.evaluate(np.ones(run_size := synth.make_problem("He", 8, 3).x.size))
+    assert f == 0.0 and run_size > 0
+    run.close()
+    assert srv.closed == [run.id]
+
+
 def test_dropped_connection_closes_the_run(endpoint):
     srv, ep = endpoint
     run = RemoteRun(ep.address, ep.authkey, synth.make_problem("H2", 6, 1))

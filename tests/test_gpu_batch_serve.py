@@ -38,7 +38,7 @@ def test_autograd_backward_is_the_gradient_kernel(torch_cuda):
     E = energy(iv, C, eng)
     (3.0 * E).backward()
     fo, go = Oracle.from_problem(p).outprod(p.x, nthreads=8)
-    assert abs(float(E) - fo) < TOL_E
+    assert abs(float(E.detach()) - fo) < TOL_E
     g = torch.cat([iv.grad, C.grad]).cpu().numpy()
     assert normwise(g, 3.0 * go) < TOL_G
 
@@ -295,3 +295,43 @@ def test_server_endpoint_remote_run(torch_cuda):
             srv.close_run(local)
         finally:
             ep.close()
+
+
+def test_server_faults_injected_on_the_host(torch_cuda):
+    """Malformed and failing requests do not disturb the server: a wrong-sized
+    x is refused at submission, a NaN parameter comes back as a status error
+    (the run stays usable), a non-positive-definite pair as LinAlgError, and a
+    request still queued when its run is closed fails instead of hanging."""
+    from nbo_correlatedgaussians_b200 import _lib, synth
+    from nbo_correlatedgaussians_b200.serve import Request, Server
+    p = synth.make_problem("H2", 40, 71)
+    with Server(max_slots=4, tune=False) as srv:
+        run = srv.open_run(p, timeout=60)
+        f0, g0 = srv.evaluate(run, p.x, timeout=60)
+        with pytest.raises(ValueError):
+            srv.evaluate(run, p.x[:-1])
+        bad = p.x.copy()
+        bad[5] = np.nan
+        with pytest.raises((_lib.NecgError, np.linalg.LinAlgError)):
+            srv.evaluate(run, bad, timeout=60)
+        npd = p.x.copy()
+        npd[3 * p.blk:3 * p.blk + p.svh] = 0.0
+        with pytest.raises(np.linalg.LinAlgError):
+            srv.evaluate(run, npd, timeout=60)
+        f1, g1 = srv.evaluate(run, p.x, timeout=60)
+        assert f1 == f0 and np.array_equal(g1, g0)
+        # a request that no step has taken yet when the run closes
+        with srv.lock:
+            held = list(srv.free_batches)
+            srv.free_batches.clear()  # hold the step loop: no plan is free
+            req = Request(run, p.x.copy())
+            srv.pending.append(req)
+        closer = threading.Thread(target=srv.close_run, args=(run,))
+        closer.start()
+        assert req.done.wait(60) and isinstance(req.error, RuntimeError)
+        closer.join(60)
+        with srv.lock:
+            srv.free_batches.extend(held)
+            srv.lock.notify_all()
+        with pytest.raises(RuntimeError):
+            srv.evaluate(run, p.x)
