@@ -15,7 +15,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libnecg_b200.so")
 SOURCES = ["necg_kernels.cu", "necg_capi.cu", "necg_count.cu", "necg_batch.cu", "necg_noalloc.cu"]
-HEADERS = ["necg_math.cuh", "necg_kernels.cuh", "necg_lanes.cuh", "necg_handle.h", "necg_hostscalar.cuh"]
+HEADERS = ["necg_math.cuh", "necg_kernels.cuh", "necg_lanes.cuh", "necg_handle.h", "necg_hostscalar.cuh",
+           "necg_device.cuh", "necg_trace.h"]
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--shared", "-cudart", "static",

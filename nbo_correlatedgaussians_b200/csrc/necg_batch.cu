@@ -28,6 +28,7 @@
 #include "necg_handle.h"
 #include "necg_lanes.cuh"
 #include "necg_math.cuh"
+#include "necg_trace.h"
 
 namespace necg {
 
@@ -562,6 +563,7 @@ int necg_batch_destroy(necg_batch *b) {
 int necg_batch_plan(necg_batch *b, int count, necg_handle *const *hs, const int *Ks,
                     const double *const *x_dev, double *const *g_dev, double *const *f_dev,
                     void *stream) {
+    necg::TraceRange trace("necg_batch_plan");
     if (!b || count < 0 || count > b->cap_inst || (count > 0 && (!hs || !Ks || !x_dev || !g_dev)))
         return NECG_ERR_ARG;
     cudaStream_t st = (cudaStream_t)stream;
@@ -695,6 +697,7 @@ int necg_batch_plan(necg_batch *b, int count, necg_handle *const *hs, const int 
 }
 
 int necg_batch_step(necg_batch *b, void *stream) {
+    necg::TraceRange trace("necg_batch_step");
     if (!b) return NECG_ERR_ARG;
     BCK(cudaSetDevice(b->device));
     launch_step(b, (cudaStream_t)stream, b->mode);
@@ -709,6 +712,7 @@ int necg_batch_graph(necg_batch *b, void *stream) {
 }
 
 int necg_batch_replay(necg_batch *b, void *stream) {
+    necg::TraceRange trace("necg_batch_replay");
     if (!b) return NECG_ERR_ARG;
     BCK(cudaSetDevice(b->device));
     const int mode = b->mode;

@@ -30,6 +30,7 @@
 #include "necg_handle.h"
 #include "necg_kernels.cuh"
 #include "necg_math.cuh"
+#include "necg_trace.h"
 
 using necg::LaunchArgs;
 
@@ -513,6 +514,7 @@ int necg_build_matrices(necg_handle *h, int K, const double *iv_dev, const doubl
 
 int necg_outprod(necg_handle *h, int K, const double *x_dev, double *f_dev, double *g_dev,
                  double *H_dev, double *S_dev, void *stream) {
+    necg::TraceRange trace("necg_outprod");
     int rc = check_K(h, K);
     if (rc) return rc;
     if (!x_dev || !g_dev) return NECG_ERR_ARG;
@@ -599,6 +601,7 @@ int necg_shard_tiles(necg_handle *h, int K, int *ntiles) {
 
 int necg_shard_pairs(necg_handle *h, int K, const double *x_dev, int tile_begin, int tile_end,
                      double *rows_dev, void *stream) {
+    necg::TraceRange trace("necg_shard_pairs");
     cudaStream_t st = (cudaStream_t)stream;
     LaunchArgs a;
     int rc = shard_args(h, K, x_dev, tile_begin, tile_end, st, a);
@@ -616,6 +619,7 @@ int necg_shard_pairs(necg_handle *h, int K, const double *x_dev, int tile_begin,
 
 int necg_shard_grad(necg_handle *h, int K, const double *x_dev, const double *rows_dev, int tile_begin,
                     int tile_end, double *f_dev, double *g_dev, double *sums_dev, void *stream) {
+    necg::TraceRange trace("necg_shard_grad");
     cudaStream_t st = (cudaStream_t)stream;
     LaunchArgs a;
     int rc = shard_args(h, K, x_dev, tile_begin, tile_end, st, a);
@@ -632,6 +636,7 @@ int necg_shard_grad(necg_handle *h, int K, const double *x_dev, const double *ro
 
 int necg_shard_finish(necg_handle *h, int K, const double *x_dev, const double *sums_dev, double *g_dev,
                       void *stream) {
+    necg::TraceRange trace("necg_shard_finish");
     int rc = check_K(h, K);
     if (rc) return rc;
     if (!x_dev || !sums_dev || !g_dev) return NECG_ERR_ARG;
@@ -649,6 +654,7 @@ int necg_shard_finish(necg_handle *h, int K, const double *x_dev, const double *
 
 int necg_outprod_host(necg_handle *h, int K, const double *x_host, double *f_host,
                       double *g_host, void *stream) {
+    necg::TraceRange trace("necg_outprod_host");
     int rc = check_K(h, K);
     if (rc) return rc;
     if (!x_host || !g_host) return NECG_ERR_ARG;
@@ -666,6 +672,7 @@ int necg_outprod_host(necg_handle *h, int K, const double *x_host, double *f_hos
 int necg_make_grad(necg_handle *h, int K, const double *iv_dev, const double *C_dev,
                    const double *H_dev, const double *S_dev, double eng, double norm,
                    double *g_dev, void *stream) {
+    necg::TraceRange trace("necg_make_grad");
     int rc = check_K(h, K);
     if (rc) return rc;
     if (!iv_dev || !C_dev || !H_dev || !S_dev || !g_dev) return NECG_ERR_ARG;
