@@ -232,6 +232,10 @@ def run_engine(args):
         tiles = dict(tuned(eng, x, prob.K))  # untimed; cached per (GPU, n, nst, K bucket)
     if args.pair_pass != "auto":
         tiles["sym"] = PASS_MODE[args.pair_pass]
+        if tiles["sym"] != 2:  # variants above 100 and the splits exist for the fused pass only
+            tiles["npc"] = 1
+            if int(tiles.get("minw_s", 8)) not in (8, 12, 16):
+                tiles["minw_s"] = 8
     apply(eng, tiles)
     _lib.check(L.necg_profile(eng.h, 1), "necg_profile")
     g = torch.empty_like(x)
@@ -353,7 +357,8 @@ def run_engine(args):
                    "pair_pass": ("fused energy + gradient, unordered pairs" if mode == 2 else
                                  "energy pass + gradient over unordered pairs" if mode == 1 else
                                  "energy pass + gradient over ordered pairs"),
-                   "tiles": {k: tiles[k] for k in ("lc_e", "minb_e", "lc_g", "minb_g", "sym", "lc_s", "minw_s")
+                   "tiles": {k: tiles.get(k, 1) for k in ("lc_e", "minb_e", "lc_g", "minb_g", "sym", "lc_s", "minw_s",
+                                                          "npc")
                              if k in tiles},
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
         "pair_elements_per_s": value * prob.pairs,

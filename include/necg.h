@@ -95,6 +95,15 @@ int necg_set_variant(necg_handle *h, int minw_energy, int minw_grad);
  * memory does not fit, n = 5).  Set by the autotuner. */
 int necg_set_symmetric(necg_handle *h, int mode, int lc, int minw);
 
+/* Fused pass (mode 2) with one-warp tiles (variants below 200): split the nst
+ * symmetry terms of every tile over npc warps, 1 <= npc <= nst (1: no split,
+ * the default).  A small basis has few tiles, each a long chain of LC x nst
+ * terms; split, its tiles fill more of the GPU.  The splits' H and S sums go to
+ * npc K x K buffers that one more kernel adds up in a fixed order.  No
+ * counterpart in the reference (its loops have no such schedule).  Set by the
+ * autotuner. */
+int necg_set_splits(necg_handle *h, int npc);
+
 /* One objective evaluation: python/outprod.py:20-76 outprod(x) -> (f, g),
  * including make_grad (python/make_grad.py:18-90).  Device pointers; H_dev and
  * S_dev (K*K) receive the symmetric matrices and may be NULL (workspace is used).

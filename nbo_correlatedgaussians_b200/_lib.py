@@ -33,6 +33,7 @@ SIGNATURES = [
     ("necg_set_tiles", _i, [_vp, _i, _i]),
     ("necg_set_variant", _i, [_vp, _i, _i]),
     ("necg_set_symmetric", _i, [_vp, _i, _i, _i]),
+    ("necg_set_splits", _i, [_vp, _i]),
     ("necg_outprod", _i, [_vp, _i, _vp, _vp, _vp, _vp, _vp, _vp]),
     ("necg_outprod_host", _i, [_vp, _i, _vp, _vp, _vp, _vp]),
     ("necg_build_matrices", _i, [_vp, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),

@@ -18,6 +18,9 @@ The search space:
          pairs, with its own ket chunk lc_s and variant minw_s; sym = 2 fuses
          it with the energy pass (one pass for H, S and both gradients), kept
          when its total beats the best separate energy + gradient passes
+  npc    splits of the symmetry terms per tile of the fused pass (one-warp
+         variants): tried when the basis has few tiles (SPLIT_TILES), where each
+         tile's chain of LC x nst terms, not the GPU's width, sets the time
 """
 from __future__ import annotations
 
@@ -40,11 +43,18 @@ MINB_GRAD_EXTRA = (112, 116)  # gradient kernel with shared-memory accumulators
 LC_S = (2, 4, 8, 16)          # kets per tile of the symmetric gradient pass
 MINW_SYM = (8, 12)
 MINW_FUSED = (8, 12, 16, 108, 112, 118, 122, 208, 218, 228, 222, 232)
+SPLITS = (1, 2, 3, 4, 6, 8, 12, 24)
+SPLIT_TILES = 2048  # try splits below this many fused tiles
 # 100 + w: ket records re-read at each use (118 / 122: staged in shared memory,
 # 8 / 12 warps); 2xy: lockstep blocks (208 8 warps,
 # 218 + bras in shared memory, 228 + ket record in shared memory, 222 / 232 the
 # same with 12 warps); a variant whose shared memory does not fit for n is refused
 # by necg_set_symmetric and skipped
+
+
+def fused_tiles(K: int, lc: int) -> int:
+    """Tiles (32-row block, chunk of lc kets) over the lower triangle of K."""
+    return sum(min(kb * 32 + 31, K - 1) // lc + 1 for kb in range((K + 31) // 32))
 
 
 def _bucket(K: int) -> int:
@@ -131,14 +141,20 @@ def tune(eng: Engine, x, K: int, reps: int = 3, report: bool = False) -> dict:
             for lc in LC_S:
                 if L.necg_set_symmetric(eng.h, 2, lc, minw) != _lib.NECG_OK:
                     continue
-                _phase_times(eng, x, K, 1)
-                t = _phase_times(eng, x, K, reps).min(axis=0)
-                tot = float(t[1] + t[3] + t[4])
-                rows.append({"sym": 2, "minw": minw, "lc_s": lc, "total_ms": tot})
-                if tot < best_sep and (fused is None or tot < fused[0]):
-                    fused = (tot, lc, minw)
+                splits = [1]
+                if minw < 200 and fused_tiles(K, lc) < SPLIT_TILES:
+                    splits = [s for s in SPLITS if s <= eng.nst]
+                for npc in splits:
+                    _lib.check(L.necg_set_splits(eng.h, npc), "necg_set_splits")
+                    _phase_times(eng, x, K, 1)
+                    t = _phase_times(eng, x, K, reps).min(axis=0)
+                    tot = float(t[1] + t[3] + t[4])
+                    rows.append({"sym": 2, "minw": minw, "lc_s": lc, "npc": npc, "total_ms": tot})
+                    if tot < best_sep and (fused is None or tot < fused[0]):
+                        fused = (tot, lc, minw, npc)
+                L.necg_set_splits(eng.h, 1)
         if fused is not None:
-            res.update(sym=2, lc_s=fused[1], minw_s=fused[2], fused_ms=fused[0])
+            res.update(sym=2, lc_s=fused[1], minw_s=fused[2], npc=fused[3], fused_ms=fused[0])
     if report:
         res["table"] = rows
     apply(eng, res)
@@ -152,6 +168,7 @@ def apply(eng: Engine, cfg: dict) -> None:
     rc = eng.L.necg_set_symmetric(eng.h, sym, int(cfg.get("lc_s", 4)), int(cfg.get("minw_s", 8)))
     if rc != _lib.NECG_OK and sym:
         _lib.check(rc, "necg_set_symmetric")
+    _lib.check(eng.L.necg_set_splits(eng.h, min(int(cfg.get("npc", 1)), eng.nst)), "necg_set_splits")
 
 
 def tuned(eng: Engine, x, K: int, retune: bool = False) -> dict:

@@ -121,7 +121,8 @@ void free_all(necg_handle *h) {
     void *ptrs[] = {h->d_sml, h->d_sms, h->d_scvv, h->d_bra, h->d_ket, h->d_part, h->d_H,
                     h->d_S, h->d_rows, h->d_scal, h->d_x, h->d_g, h->d_f, h->d_status,
                     h->d_tiles, h->d_pinv, h->d_kcnt, h->d_ksrc, h->d_kcoef, h->d_stiles,
-                    h->d_stile_start, h->d_psym, h->d_sgroups, h->d_qcount, h->d_bgroups};
+                    h->d_stile_start, h->d_psym, h->d_sgroups, h->d_qcount, h->d_bgroups,
+                    h->d_Hp, h->d_Sp};
     for (void *p : ptrs) pool_free(h, p);
 }
 
@@ -148,14 +149,31 @@ int ensure_tiles(necg_handle *h, int K, cudaStream_t st) {
     return NECG_OK;
 }
 
+// Splits of the symmetry terms the fused pass uses per one-warp tile (1: none).
+int fused_splits(const necg_handle *h) { return h->grad_mode == 2 && h->minb_s < 200 && h->npc > 1 ? h->npc : 1; }
+
 // Lower-triangle tiles of chunk LC for the symmetric pass, plus the first tile
 // of each 32-row block; the partial buffer grows here if this K and LC need more.
-// mult = 2 for the fused pass (H and S partials kept apart), 1 otherwise.
+// mult = 2 for the fused pass (H and S partials kept apart), 1 otherwise; the
+// fused pass with npc splits needs npc partial slots per tile and npc K x K
+// buffers for H and S.
 int ensure_sym_tiles(necg_handle *h, int K, cudaStream_t st, int mult) {
     const int PS = necg::part_stride(h->n);
     const int gw = necg::fused_block_warps(h->minb_s);  // tiles per group of the lockstep-block pass
+    const int npc = mult == 2 ? fused_splits(h) : 1;
+    const size_t hp_need = npc > 1 ? (size_t)npc * K * K : 0;
+    if (hp_need > h->hp_cap) {
+        pool_free(h, h->d_Hp, st);
+        pool_free(h, h->d_Sp, st);
+        h->d_Hp = h->d_Sp = nullptr;
+        h->hp_cap = 0;
+        CK(pool_alloc(h, &h->d_Hp, hp_need * sizeof(double), st));
+        CK(pool_alloc(h, &h->d_Sp, hp_need * sizeof(double), st));
+        h->ws_bytes += (long long)(2 * hp_need * sizeof(double));
+        h->hp_cap = hp_need;
+    }
     if (h->stiles_K == K && h->stiles_lc == h->lc_s && h->sgroups_w == gw &&
-        (size_t)h->nstiles * PS * (32 + h->lc_s) * mult <= h->psym_cap)
+        (size_t)h->nstiles * PS * (32 + h->lc_s) * mult * npc <= h->psym_cap)
         return NECG_OK;
     std::vector<int2> t;
     std::vector<int> start;
@@ -173,7 +191,7 @@ int ensure_sym_tiles(necg_handle *h, int K, cudaStream_t st, int mult) {
         h->stiles_cap = (int)t.size();
     }
     if (!h->d_stile_start) CK(pool_alloc(h, &h->d_stile_start, ((h->K_max + 31) / 32 + 2) * sizeof(int), st));
-    const size_t need = t.size() * (size_t)PS * (32 + LC) * mult;
+    const size_t need = t.size() * (size_t)PS * (32 + LC) * mult * npc;
     if (need > h->psym_cap) {
         pool_free(h, h->d_psym, st);
         h->d_psym = nullptr;
@@ -481,6 +499,12 @@ int necg_set_symmetric(necg_handle *h, int mode, int lc, int minw) {
     return NECG_OK;
 }
 
+int necg_set_splits(necg_handle *h, int npc) {
+    if (!h || npc < 1 || npc > h->nst) return NECG_ERR_ARG;
+    h->npc = npc;
+    return NECG_OK;
+}
+
 int necg_set_variant(necg_handle *h, int minw_energy, int minw_grad) {
     auto okw = [](int w) { return w == 8 || w == 12 || w == 16 || w == 20; };
     if (!h || !okw(minw_energy) || !(okw(minw_grad) || minw_grad == 112 || minw_grad == 116))
@@ -539,10 +563,14 @@ int necg_outprod(necg_handle *h, int K, const double *x_dev, double *f_dev, doub
         a.sgroups = h->d_sgroups;
         a.nsgroups = h->nsgroups;
         a.qcount = h->d_qcount;
+        a.npc = fused_splits(h);
+        a.Hp = h->d_Hp;
+        a.Sp = h->d_Sp;
         mark(h, 0, st);
         if (necg::launch_prep(a, st)) return NECG_ERR_UNSUPPORTED;
         mark(h, 1, st);
         if (necg::launch_fsym(a, st)) return NECG_ERR_ARG;
+        if (necg::launch_hs_reduce(a, st)) return NECG_ERR_ARG;
         mark(h, 2, st);
         necg::launch_rows_finalize(a, f_dev, g_dev + siv, 0, 0.0, 0.0, st);
         mark(h, 3, st);

@@ -63,6 +63,9 @@ struct FusedSmem {
 // read there instead of from global memory.
 // SKET: each (l, P) ket record is copied by the warp into sm.sket and read
 // there.
+// [p0, p1): the symmetry terms this tile takes (p1 < 0: all nst).  A pass whose
+// tiles split the terms writes each split's partials to its own slot (t is then
+// the slot index) and each split's H, S sums to its own K x K buffer.
 template <int N, bool VKET, bool BSYNC = false, bool SBRA = false, bool SKET = false>
 __device__ __forceinline__ void fsym_tile(int t, int2 tl, int LC, int K, int nst, const Consts<N> &cs,
                                           const double *__restrict__ bra, const double *__restrict__ ket,
@@ -70,7 +73,7 @@ __device__ __forceinline__ void fsym_tile(int t, int2 tl, int LC, int K, int nst
                                           double *__restrict__ H, double *__restrict__ S,
                                           double *__restrict__ part_b, double *__restrict__ part_k,
                                           int *status, FusedSmem sm, bool idle = false,
-                                          const double *sbra = nullptr) {
+                                          const double *sbra = nullptr, int p0 = 0, int p1 = -1) {
     using KL = KetLayout<N>;
     constexpr int PS = Part<N>::size;
     static_assert(PS <= 32, "the symmetric pass needs tri(n) + 1 + 3n <= 32");
@@ -105,7 +108,8 @@ __device__ __forceinline__ void fsym_tile(int t, int2 tl, int LC, int K, int nst
         double aH = 0.0, aS = 0.0, hsum = 0.0, ssum = 0.0;
         const bool active = kval && l <= k && lok;
         const BraRef b{bra + (active ? k : (lok ? l : 0)), (size_t)K};
-        for (int P = 0; P < nst; ++P) {
+        const int pend = p1 < 0 ? nst : p1;
+        for (int P = p0; P < pend; ++P) {
             if (BSYNC && !lok) {
                 __syncthreads();
                 continue;

@@ -43,6 +43,10 @@ struct necg_handle {
     int *d_qcount = nullptr;    // queue head of the block-synchronised fused pass
     int2 *d_bgroups = nullptr;  // the same groups with 8 chunks each (the batched step's blocks)
     int bgroups_cap = 0, nbgroups = 0;
+    // fused pass with one-warp tiles: symmetry terms split over npc warps per tile
+    int npc = 1;
+    double *d_Hp = nullptr, *d_Sp = nullptr;  // npc K x K sums each
+    size_t hp_cap = 0;                        // doubles per buffer
 };
 
 namespace necg {

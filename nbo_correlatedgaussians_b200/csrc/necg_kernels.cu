@@ -273,9 +273,13 @@ __global__ void __launch_bounds__(32, MINW) gsym_kernel(const int2 *__restrict__
 
 // Fused pass over unordered pairs (k >= l): one warp per tile; the body is
 // fsym_tile (necg_device.cuh), shared with the batched persistent kernel.
+// blockIdx.y = pc splits the symmetry terms of every tile over npc warps (a
+// small basis then still fills the GPU): split pc takes terms [pc PC, pc PC +
+// PC), writes its partials to slot t npc + pc and its H, S sums to H, S + pc K^2
+// (to be summed by hs_reduce_kernel); npc = 1 is the unsplit pass.
 template <int N, int MINW, bool VKET, bool SKET>
 __global__ void __launch_bounds__(32, MINW) fsym_kernel(const int2 *__restrict__ tiles, int t_begin, int t_end,
-                                                   int LC, int K, int nst, Consts<N> cs,
+                                                   int LC, int K, int nst, int npc, Consts<N> cs,
                                                    const double *__restrict__ bra,
                                                    const double *__restrict__ ket,
                                                    const double *__restrict__ C, KetMap kmap,
@@ -288,8 +292,27 @@ __global__ void __launch_bounds__(32, MINW) fsym_kernel(const int2 *__restrict__
     __shared__ double sket[SKET ? KetLayout<N>::size : 2];
     const int t = t_begin + blockIdx.x;
     if (t >= t_end) return;
-    fsym_tile<N, VKET, false, false, SKET>(t, tiles[t], LC, K, nst, cs, bra, ket, C, kmap, H, S, part_b, part_k,
-                                           status, FusedSmem{sacc, krow, kred, sket});
+    const int pc = blockIdx.y, PC = (nst + npc - 1) / npc;
+    const int p0 = min(pc * PC, nst), p1 = min(p0 + PC, nst);
+    const size_t off = (size_t)pc * K * K;
+    fsym_tile<N, VKET, false, false, SKET>(t * npc + pc, tiles[t], LC, K, nst, cs, bra, ket, C, kmap, H + off,
+                                           S + off, part_b, part_k, status, FusedSmem{sacc, krow, kred, sket},
+                                           false, nullptr, p0, p1);
+}
+
+// H, S = sum over the npc splits of the fused pass (fixed order: deterministic).
+__global__ void __launch_bounds__(256) hs_reduce_kernel(const double *__restrict__ Hp,
+                                                        const double *__restrict__ Sp, int npc, size_t KK,
+                                                        double *__restrict__ H, double *__restrict__ S) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < KK; i += (size_t)gridDim.x * blockDim.x) {
+        double h = Hp[i], s = Sp[i];
+        for (int pc = 1; pc < npc; ++pc) {
+            h += Hp[pc * KK + i];
+            s += Sp[pc * KK + i];
+        }
+        H[i] = h;
+        S[i] = s;
+    }
 }
 
 // The fused pass with W-warp blocks (W = 8 or 12), one per SM, persistent over
@@ -363,13 +386,14 @@ __global__ void __launch_bounds__(256) fsym_sum_kernel(const int *__restrict__ t
                                                        const double *__restrict__ part_b,
                                                        const double *__restrict__ part_k,
                                                        const double *__restrict__ scal,
-                                                       double *__restrict__ out, int t0, int t1) {
+                                                       double *__restrict__ out, int t0, int t1, int npc) {
     constexpr int PS = Part<N>::size;
     __shared__ double red[2][8][32];
     const int kb = blockIdx.x, f = blockIdx.y;
     const int lane = threadIdx.x & 31, seg = threadIdx.x >> 5;
     const int m = kb * 32 + lane;
-    const int ta = max(tstart[kb], t0), tb = min(tstart[kb + 1], t1);
+    // partial slots: tile t's splits are slots t npc .. t npc + npc - 1
+    const int ta = max(tstart[kb], t0) * npc, tb = min(tstart[kb + 1], t1) * npc;
     double sH = 0.0, sS = 0.0;
     for (int t = ta + seg; t < tb; t += 8) {
         sH += part_b[(((size_t)t * 2 + 0) * PS + f) * 32 + lane];
@@ -393,9 +417,11 @@ __global__ void __launch_bounds__(256) fsym_sum_kernel(const int *__restrict__ t
     for (int q = kb0; q < nkb; ++q) {
         const int t = tstart[q] + lc;
         if (t < t0 || t >= t1) continue;
-        const size_t base = ((size_t)t * LC + ll) * 2;
-        sH += part_k[(base + 0) * PS + f];
-        sS += part_k[(base + 1) * PS + f];
+        for (int pc = 0; pc < npc; ++pc) {
+            const size_t base = ((size_t)(t * npc + pc) * LC + ll) * 2;
+            sH += part_k[(base + 0) * PS + f];
+            sS += part_k[(base + 1) * PS + f];
+        }
     }
     out[(size_t)f * K + m] = sH - scal[0] * sS;
 }
@@ -733,9 +759,10 @@ template <int N> struct Launch {
             Consts<N> cs = make_consts<N>(a.mass_h, a.ncv_h, a.efs);
             const int t0 = a.st_end > 0 ? a.st_begin : 0, t1 = a.st_end > 0 ? a.st_end : a.nstiles;
             if (t1 <= t0) return;
-            fsym_kernel<N, MINW, VKET, SKET><<<t1 - t0, 32, 0, st>>>(
-                a.stiles, t0, t1, a.LC_s, a.K, a.nst, cs, a.bra, a.ket, a.C, a.kmap, a.H, a.S, a.psym,
-                a.psym + (size_t)a.nstiles * 2 * Part<N>::size * 32, a.status);
+            const int npc = a.npc > 1 ? a.npc : 1;
+            fsym_kernel<N, MINW, VKET, SKET><<<dim3(t1 - t0, npc), 32, 0, st>>>(
+                a.stiles, t0, t1, a.LC_s, a.K, a.nst, npc, cs, a.bra, a.ket, a.C, a.kmap, npc > 1 ? a.Hp : a.H,
+                npc > 1 ? a.Sp : a.S, a.psym, a.psym + (size_t)a.nstiles * npc * 2 * Part<N>::size * 32, a.status);
         }
     }
     template <bool SBRA, bool SKET, int WARPS> static void fsym_block(const LaunchArgs &a, cudaStream_t st) {
@@ -787,9 +814,10 @@ template <int N> struct Launch {
         if constexpr (Part<N>::size <= 32) {
             constexpr int PS = Part<N>::size;
             const int t0 = a.st_end > 0 ? a.st_begin : 0, t1 = a.st_end > 0 ? a.st_end : a.nstiles;
+            const int npc = a.npc > 1 && a.minb_s < 200 ? a.npc : 1;
             fsym_sum_kernel<N><<<dim3((a.K + 31) / 32, PS), 256, 0, st>>>(
-                a.stile_start, a.LC_s, a.K, a.psym, a.psym + (size_t)a.nstiles * 2 * PS * 32, a.scal,
-                a.sums ? a.sums : a.part, t0, t1);
+                a.stile_start, a.LC_s, a.K, a.psym, a.psym + (size_t)a.nstiles * npc * 2 * PS * 32, a.scal,
+                a.sums ? a.sums : a.part, t0, t1, npc);
             if (!a.sums)
                 grad_reduce_kernel<N><<<(a.K + 127) / 128, 128, 0, st>>>(a.part, a.K, a.bra, a.C, a.scal, a.g,
                                                                           a.status);
@@ -891,6 +919,14 @@ int launch_fsym_reduce(const LaunchArgs &a, cudaStream_t st) {
     if (a.n > 5) return -1;
     if (!a.stile_start || !a.psym || !a.scal || (!a.sums && (!a.part || !a.bra || !a.C || !a.g))) return -1;
     NECG_DISPATCH(a.n, fsym_reduce(a, st));
+    return 0;
+}
+int launch_hs_reduce(const LaunchArgs &a, cudaStream_t st) {
+    if (a.npc <= 1) return 0;
+    if (!a.Hp || !a.Sp || !a.H || !a.S) return -1;
+    const size_t KK = (size_t)a.K * a.K;
+    const size_t blocks = (KK + 255) / 256 < 4096 ? (KK + 255) / 256 : 4096;
+    hs_reduce_kernel<<<(int)blocks, 256, 0, st>>>(a.Hp, a.Sp, a.npc, KK, a.H, a.S);
     return 0;
 }
 int launch_reduce_sums(const LaunchArgs &a, const double *sums, cudaStream_t st) {

@@ -35,6 +35,10 @@ struct LaunchArgs {
     const int2 *sgroups;                   // (kb, first lc)
     int nsgroups;
     int *qcount;                           // group queue head (reset before the launch)
+    // fused pass with the symmetry terms split over npc tiles per (kb, lc) (one-warp
+    // variants; npc <= 1: no split): split pc writes its H, S sums to Hp, Sp + pc K^2
+    int npc;
+    double *Hp, *Sp;
 };
 
 int launch_prep(const LaunchArgs &a, cudaStream_t st);
@@ -50,6 +54,8 @@ int launch_fsym(const LaunchArgs &a, cudaStream_t st);
 int fused_block_warps(int variant);
 bool fused_variant_ok(int n, int variant);
 int launch_fsym_reduce(const LaunchArgs &a, cudaStream_t st);
+// H, S = sum over the splits of Hp, Sp (fused pass with npc > 1), before rows/finalize
+int launch_hs_reduce(const LaunchArgs &a, cudaStream_t st);
 int launch_grad_tiles(const LaunchArgs &a, cudaStream_t st);
 int launch_grad_reduce(const LaunchArgs &a, cudaStream_t st);
 int launch_matel(const LaunchArgs &a, const int *terms, int nterms, double *out, cudaStream_t st);

@@ -252,6 +252,59 @@ def test_fused_pass_matches_oracle(torch_cuda, system, K, lc):
         assert np.max(np.abs(Sn - Sr)) <= TOL_ELEM * max(1.0, np.max(np.abs(Sr)))
 
 
+@pytest.mark.parametrize("system,K,lc", [("He", 40, 2), ("H2", 33, 1), ("LiH", 12, 2), ("LiH", 70, 4)])
+def test_fused_pass_split_terms(torch_cuda, system, K, lc):
+    """The fused pass with the symmetry terms of each tile split over npc warps
+    (necg_set_splits): E, g, H and S against the oracle and against the unsplit
+    pass for every split count, one-warp variants; lockstep variants ignore
+    the setting."""
+    import torch
+    from nbo_correlatedgaussians_b200 import _lib, synth
+    p = synth.make_problem(system, K, 5 * K + 1)
+    p.C = np.random.default_rng(K + 1).normal(size=K)
+    eng = _engine(p)
+    L = eng.L
+    fr, gr, Hr, Sr = Oracle.from_problem(p).outprod(p.x, nthreads=8, return_hs=True)
+    for minw in (8, 118, 122):
+        assert L.necg_set_symmetric(eng.h, 2, lc, minw) == _lib.NECG_OK
+        assert L.necg_set_splits(eng.h, 1) == _lib.NECG_OK
+        f1, g1 = eng.outprod(p.x)
+        for npc in sorted({q for q in (2, 3, p.nst // 2, p.nst) if 1 <= q <= p.nst}):
+            assert L.necg_set_splits(eng.h, npc) == _lib.NECG_OK
+            H = torch.empty((K, K), dtype=torch.float64, device=eng.device)
+            S = torch.empty_like(H)
+            fd, gd = eng.outprod_device(torch.from_numpy(p.x), K, H=H, S=S)
+            torch.cuda.synchronize()
+            eng.raise_status("outprod")
+            f2, g2 = float(fd.item()), gd.cpu().numpy()
+            assert abs(f2 - fr) < TOL_E and normwise(g2, gr) < TOL_G
+            assert abs(f2 - f1) < 1e-12 * max(1.0, abs(f1)) and normwise(g2, g1) < 1e-12
+            Hn, Sn = H.cpu().numpy(), S.cpu().numpy()
+            assert np.array_equal(Hn, Hn.T) and np.array_equal(Sn, Sn.T)
+            assert np.max(np.abs(Hn - Hr)) <= TOL_ELEM * max(1.0, np.max(np.abs(Hr)))
+            assert np.max(np.abs(Sn - Sr)) <= TOL_ELEM * max(1.0, np.max(np.abs(Sr)))
+            f3, g3 = eng.outprod(p.x)  # deterministic: fixed summation order
+            assert f3 == f2 and np.array_equal(g3, g2)
+    assert L.necg_set_splits(eng.h, 0) == _lib.NECG_ERR_ARG
+    assert L.necg_set_splits(eng.h, p.nst + 1) == _lib.NECG_ERR_ARG
+    assert L.necg_set_symmetric(eng.h, 2, lc, 218) == _lib.NECG_OK
+    assert L.necg_set_splits(eng.h, 1) == _lib.NECG_OK
+    fb, gb = eng.outprod(p.x)
+    assert L.necg_set_splits(eng.h, 2) == _lib.NECG_OK
+    fb2, gb2 = eng.outprod(p.x)
+    assert fb2 == fb and np.array_equal(gb2, gb)
+    # the pair-status path with splits: the first failing pair and a usable handle
+    assert L.necg_set_symmetric(eng.h, 2, lc, 118) == _lib.NECG_OK
+    assert L.necg_set_splits(eng.h, min(4, p.nst)) == _lib.NECG_OK
+    bad = p.copy()
+    bad.iv[2 * p.blk:2 * p.blk + p.svh] = 0.0
+    with pytest.raises(np.linalg.LinAlgError):
+        eng.outprod(bad.x)
+    assert eng.status()[1] == 2 * K + 2
+    f4, g4 = eng.outprod(p.x)
+    assert abs(f4 - fr) < TOL_E and normwise(g4, gr) < TOL_G
+
+
 @pytest.mark.parametrize("minw", [8, 118, 208, 228])
 def test_fused_pass_oldquit_and_errors(torch_cuda, minw):
     """The fused mode on the reference's input file, and the pair-status path
