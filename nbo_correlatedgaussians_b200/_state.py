@@ -36,6 +36,9 @@ def engine() -> Engine:
         if eng is not None:
             eng.close()
         eng = Engine(p, K_max=p.K)
+        # the autotuner's setting for this (GPU, n, nst, K bucket): timed once, then cached
+        from .autotune import tuned
+        tuned(eng, p.x, p.K)
         _cache["engine"] = eng
         _cache["key"] = key
     return eng
