@@ -46,8 +46,10 @@ struct InstDesc {
     const int *pinv, *stile_start;
     const int2 *stiles;  // the instance's fused tile list (kb, lc), on the device
     const int2 *bgroups; // groups of 8 consecutive chunks of one row block (kb, first lc)
-    int nbgroups, pad2;
+    int nbgroups;
+    int npc;             // one-warp fused kernel: symmetry terms split npc ways per tile
     double *psym;
+    double *Hp, *Sp;     // npc > 1: the splits' H, S sums (npc K x K each)
     KetMap kmap;
     double cs[kConstsDoubles];
 };
@@ -179,12 +181,16 @@ __global__ void __launch_bounds__(32, 8) batch_fused_warp_kernel(PlanPtrs p) {
         if (t >= nf) break;
         const int j = find_inst(p.pref_ft, p.hdr->ninst, t);
         const InstDesc &d = p.inst[p.order[j]];
-        const int ti = t - p.pref_ft[j];  // tile index within the instance
+        const int slot = t - p.pref_ft[j];  // tile ti, split pc of the instance
+        const int npc = d.npc, ti = slot / npc, pc = slot - ti * npc;
+        const int PC = (d.nst + npc - 1) / npc, p0 = min(pc * PC, d.nst), p1 = min(p0 + PC, d.nst);
         const size_t PSd = (size_t)(tri(d.n) + 1 + 3 * d.n);
-        double *part_b = d.psym, *part_k = d.psym + (size_t)d.nstiles * 2 * PSd * 32;
-        BATCH_SWITCH(d.n, (fsym_tile<N, true>(ti, d.stiles[ti], d.lc_s, d.K, d.nst, consts_of<N>(d), d.bra,
-                                              d.ket, d.C, d.kmap, d.H, d.S, part_b, part_k, d.status,
-                                              FusedSmem{sacc, krow, kred, nullptr})));
+        double *part_b = d.psym, *part_k = d.psym + (size_t)d.nstiles * npc * 2 * PSd * 32;
+        double *H = npc > 1 ? d.Hp + (size_t)pc * d.K * d.K : d.H;
+        double *S = npc > 1 ? d.Sp + (size_t)pc * d.K * d.K : d.S;
+        BATCH_SWITCH(d.n, (fsym_tile<N, true>(slot, d.stiles[ti], d.lc_s, d.K, d.nst, consts_of<N>(d), d.bra,
+                                              d.ket, d.C, d.kmap, H, S, part_b, part_k, d.status,
+                                              FusedSmem{sacc, krow, kred, nullptr}, false, nullptr, p0, p1)));
     }
 }
 
@@ -242,6 +248,26 @@ __global__ void __launch_bounds__(256, 1) batch_fused_kernel(PlanPtrs p) {
     }
 }
 
+// H, S of every instance whose symmetry terms were split: the sum over its
+// splits, in a fixed order (before rows / finalize read them).
+__global__ void __launch_bounds__(256) batch_hs_reduce_kernel(PlanPtrs p) {
+    const int ninst = p.hdr->ninst;
+    for (int q = 0; q < ninst; ++q) {
+        const InstDesc &d = p.inst[q];
+        if (d.npc <= 1) continue;
+        const size_t KK = (size_t)d.K * d.K;
+        for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < KK; i += (size_t)gridDim.x * blockDim.x) {
+            double h = d.Hp[i], s = d.Sp[i];
+            for (int pc = 1; pc < d.npc; ++pc) {
+                h += d.Hp[pc * KK + i];
+                s += d.Sp[pc * KK + i];
+            }
+            d.H[i] = h;
+            d.S[i] = s;
+        }
+    }
+}
+
 // g_H - E g_S of every instance into its part (field-major, chunk 0).
 __global__ void __launch_bounds__(256) batch_fsum_kernel(PlanPtrs p) {
     const int ninst = p.hdr->ninst;
@@ -252,9 +278,11 @@ __global__ void __launch_bounds__(256) batch_fsum_kernel(PlanPtrs p) {
         const int id = i - p.pref_sum[q];
         const int f = id / d.K, m = id - f * d.K;
         const size_t PSd = (size_t)(tri(d.n) + 1 + 3 * d.n);
-        const double *part_b = d.psym, *part_k = d.psym + (size_t)d.nstiles * 2 * PSd * 32;
+        const int npc = d.npc > 1 ? d.npc : 1;
+        const double *part_b = d.psym, *part_k = d.psym + (size_t)d.nstiles * npc * 2 * PSd * 32;
         double v = 0.0;
-        BATCH_SWITCH(d.n, v = fsym_sum_one<N>(d.stile_start, d.lc_s, d.K, f, m, part_b, part_k, d.scal[0]));
+        BATCH_SWITCH(d.n, v = fsym_sum_one<N>(d.stile_start, d.lc_s, d.K, f, m, part_b, part_k, d.scal[0], 0,
+                                              0x7fffffff, npc));
         d.part[(size_t)f * d.K + m] = v;
     }
 }
@@ -473,8 +501,12 @@ void launch_step(necg_batch *b, cudaStream_t st, int mode) {
     batch_reset_kernel<<<1, 256, 0, st>>>(p);
     batch_prep_kernel<<<g * 4, 128, 0, st>>>(p);
     if (mode) {
-        if (mode == 2) batch_fused_warp_kernel<<<g * b->occ_fwarp, 32, 0, st>>>(p);
-        else batch_fused_kernel<<<g, 256, kBatchFusedSmem, st>>>(p);
+        if (mode == 2) {
+            batch_fused_warp_kernel<<<g * b->occ_fwarp, 32, 0, st>>>(p);
+            batch_hs_reduce_kernel<<<g * 2, 256, 0, st>>>(p);
+        } else {
+            batch_fused_kernel<<<g, 256, kBatchFusedSmem, st>>>(p);
+        }
         batch_rows_kernel<<<g * 4, 256, 0, st>>>(p);
         batch_finalize_kernel<<<g, 256, 0, st>>>(p);
         batch_fsum_kernel<<<g * 4, 256, 0, st>>>(p);
@@ -631,6 +663,9 @@ int necg_batch_plan(necg_batch *b, int count, necg_handle *const *hs, const int 
             d.stiles = h->d_stiles;
             d.bgroups = h->d_bgroups;
             d.nbgroups = h->nbgroups;
+            d.npc = 1;  // set below for the one-warp kernel
+            d.Hp = h->d_Hp;
+            d.Sp = h->d_Sp;
         }
         const int ps = tri(n) + 1 + 3 * n;
         hp.pref_bra[q + 1] = hp.pref_bra[q] + K;
@@ -657,10 +692,14 @@ int necg_batch_plan(necg_batch *b, int count, necg_handle *const *hs, const int 
         long long ng = 0;
         for (int q = 0; q < count; ++q) ng += hp.inst[q].nbgroups;
         fine = ng < 4LL * b->sms;  // too few groups to fill the SMs with 8-warp blocks
+        // the one-warp kernel splits each instance's symmetry terms as its handle does
+        // (its partial buffers and H, S split buffers are sized for that)
+        if (fine)
+            for (int q = 0; q < count; ++q) hp.inst[q].npc = fused_splits(hs[q]);
         hp.pref_ft[0] = 0;
         for (int j = 0; j < count; ++j) {
             const InstDesc &dj = hp.inst[hp.order[j]];
-            nf += fine ? dj.nstiles : dj.nbgroups;
+            nf += fine ? (long long)dj.nstiles * dj.npc : dj.nbgroups;
             if (nf > 0x7fffffff) return NECG_ERR_CAPACITY;
             hp.pref_ft[j + 1] = (int)nf;
         }

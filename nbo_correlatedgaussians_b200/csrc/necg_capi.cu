@@ -149,9 +149,6 @@ int ensure_tiles(necg_handle *h, int K, cudaStream_t st) {
     return NECG_OK;
 }
 
-// Splits of the symmetry terms the fused pass uses per one-warp tile (1: none).
-int fused_splits(const necg_handle *h) { return h->grad_mode == 2 && h->minb_s < 200 && h->npc > 1 ? h->npc : 1; }
-
 // Lower-triangle tiles of chunk LC for the symmetric pass, plus the first tile
 // of each 32-row block; the partial buffer grows here if this K and LC need more.
 // mult = 2 for the fused pass (H and S partials kept apart), 1 otherwise; the
@@ -160,7 +157,7 @@ int fused_splits(const necg_handle *h) { return h->grad_mode == 2 && h->minb_s <
 int ensure_sym_tiles(necg_handle *h, int K, cudaStream_t st, int mult) {
     const int PS = necg::part_stride(h->n);
     const int gw = necg::fused_block_warps(h->minb_s);  // tiles per group of the lockstep-block pass
-    const int npc = mult == 2 ? fused_splits(h) : 1;
+    const int npc = mult == 2 ? necg::fused_splits(h) : 1;
     const size_t hp_need = npc > 1 ? (size_t)npc * K * K : 0;
     if (hp_need > h->hp_cap) {
         pool_free(h, h->d_Hp, st);
@@ -563,7 +560,7 @@ int necg_outprod(necg_handle *h, int K, const double *x_dev, double *f_dev, doub
         a.sgroups = h->d_sgroups;
         a.nsgroups = h->nsgroups;
         a.qcount = h->d_qcount;
-        a.npc = fused_splits(h);
+        a.npc = necg::fused_splits(h);
         a.Hp = h->d_Hp;
         a.Sp = h->d_Sp;
         mark(h, 0, st);

@@ -191,16 +191,19 @@ __device__ __forceinline__ void fsym_tile(int t, int2 tl, int LC, int K, int nst
 // Sum of the fused-pass partials of basis m for field f: its bra partials from
 // the tiles of block kb = m / 32 (lane m % 32) and its ket partials from the
 // tiles of chunk lc = m / LC in every block kb' >= that chunk; returns
-// sum_H - E sum_S.  Only tiles in [t0, t1) count (a shard of the pass).
+// sum_H - E sum_S.  Only tiles in [t0, t1) count (a shard of the pass).  With
+// the symmetry terms split npc ways, tile t's partials are slots t npc ..
+// t npc + npc - 1.
 template <int N>
 __device__ __forceinline__ double fsym_sum_one(const int *__restrict__ tstart, int LC, int K, int f, int m,
                                                const double *__restrict__ part_b,
                                                const double *__restrict__ part_k, double E, int t0 = 0,
-                                               int t1 = 0x7fffffff) {
+                                               int t1 = 0x7fffffff, int npc = 1) {
     constexpr int PS = Part<N>::size;
     const int kb = m >> 5, lane = m & 31;
     double sH = 0.0, sS = 0.0;
-    for (int t = max(tstart[kb], t0); t < min(tstart[kb + 1], t1); ++t) {
+    const int sa = max(tstart[kb], t0) * npc, sb = min(tstart[kb + 1], t1) * npc;
+    for (int t = sa; t < sb; ++t) {
         sH += part_b[(((size_t)t * 2 + 0) * PS + f) * 32 + lane];
         sS += part_b[(((size_t)t * 2 + 1) * PS + f) * 32 + lane];
     }
@@ -211,9 +214,11 @@ __device__ __forceinline__ double fsym_sum_one(const int *__restrict__ tstart, i
     for (int q = kb0; q < nkb; ++q) {
         const int t = tstart[q] + lc;
         if (t < t0 || t >= t1) continue;
-        const size_t base = ((size_t)t * LC + ll) * 2;
-        sH += part_k[(base + 0) * PS + f];
-        sS += part_k[(base + 1) * PS + f];
+        for (int pc = 0; pc < npc; ++pc) {
+            const size_t base = ((size_t)(t * npc + pc) * LC + ll) * 2;
+            sH += part_k[(base + 0) * PS + f];
+            sS += part_k[(base + 1) * PS + f];
+        }
     }
     return sH - E * sS;
 }

@@ -54,4 +54,9 @@ namespace necg {
 // (the handle's ket chunk lc_s), as the batched step needs them; returns a
 // status code.  May synchronise `st` when the list changes.
 int prepare_fused(necg_handle *h, int K, cudaStream_t st);
+// Splits of the symmetry terms per one-warp tile of the fused pass (1: none):
+// npc when the handle runs the fused pass with a one-warp variant, else 1.
+inline int fused_splits(const necg_handle *h) {
+    return h->grad_mode == 2 && h->minb_s < 200 && h->npc > 1 ? h->npc : 1;
+}
 }  // namespace necg

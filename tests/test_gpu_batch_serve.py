@@ -142,6 +142,36 @@ def test_batch_modes_fused_and_ordered(torch_cuda):
                 res[i] = (f, g)
 
 
+def test_batch_split_terms(torch_cuda):
+    """Instances whose handles split the fused pass's symmetry terms
+    (necg_set_splits) in the batched one-warp step, mixed with unsplit ones:
+    against the oracle and the per-call path, and bitwise the same alone and
+    in the mix."""
+    from nbo_correlatedgaussians_b200 import _lib
+    from nbo_correlatedgaussians_b200.batch import BatchEngine
+    probs = _mixed(50)
+    be = BatchEngine(probs, tune=False)
+    splits = [2, 1, 3, 2, 4]
+    for eng, p, npc in zip(be.engines, probs, splits):
+        assert eng.L.necg_set_symmetric(eng.h, 2, 2, 118) == _lib.NECG_OK
+        assert eng.L.necg_set_splits(eng.h, min(npc, p.nst)) == _lib.NECG_OK
+    be.plan()
+    be.step(graph=True)
+    be.check()
+    res = [be.results(i) for i in range(len(probs))]
+    for i, (p, (f, g)) in enumerate(zip(probs, res)):
+        fo, go = Oracle.from_problem(p).outprod(p.x, nthreads=8)
+        assert abs(f - fo) < TOL_E and normwise(g, go) < TOL_G
+        fs, gs = be.engines[i].outprod(p.x)
+        assert abs(f - fs) < 1e-12 * abs(fs) and normwise(g, gs) < 1e-12
+    be.plan([3, 0])
+    be.step(graph=True)
+    be.check()
+    for i in (3, 0):
+        fi, gi = be.results(i)
+        assert fi == res[i][0] and np.array_equal(gi, res[i][1])
+
+
 @pytest.mark.parametrize("big", [False, True])
 def test_batch_failing_instance_is_isolated(torch_cuda, big):
     """One instance with a singular A_k + A_l' in a batched step: its status is
