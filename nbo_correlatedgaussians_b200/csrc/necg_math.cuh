@@ -364,6 +364,31 @@ NECG_HD void sandwich(const R (&Bi)[tri(N)], const R (&Mt)[tri(N)], OUT &&add) {
     }
 }
 
+// The same with each output's sum started from seed(t) (an accumulator's value,
+// so the products fuse into it): put(t, seed(t) + (Bi Mt Bi)_t).
+#pragma nv_exec_check_disable
+template <int N, typename R, typename SEED, typename OUT>
+NECG_HD void sandwich_seeded(const R (&Bi)[tri(N)], const R (&Mt)[tri(N)], SEED &&seed, OUT &&put) {
+#pragma unroll
+    for (int j = 0; j < N; ++j) {
+        R col[N];
+#pragma unroll
+        for (int a = 0; a < N; ++a) {
+            R s = Mt[sx(a, 0)] * Bi[sx(0, j)];
+#pragma unroll
+            for (int k = 1; k < N; ++k) s += Mt[sx(a, k)] * Bi[sx(k, j)];
+            col[a] = s;
+        }
+#pragma unroll
+        for (int i = j; i < N; ++i) {
+            R s = seed(sx(i, j));
+#pragma unroll
+            for (int a = 0; a < N; ++a) s += Bi[sx(i, a)] * col[a];
+            put(sx(i, j), s);
+        }
+    }
+}
+
 // B = A_k + A_l', its inverse, T = Bi (A_k S_k + A_l' S_l') and the overlap.
 #pragma nv_exec_check_disable
 template <int N, typename R, typename BA, typename KA>
@@ -750,14 +775,15 @@ NECG_HD bool term_fused(const BA &b, const KA &kr, const Consts<N> &cs, R wb, R 
         const R fb = 1.5 * Fb, fk = 1.5 * Fk, sb = 1.5 * ovb, sk = 1.5 * ovk;
 #pragma unroll
         for (int t = 0; t < tri(N); ++t) Mt[t] = ovb * (6.0 * kr[KL::Np + t] + W[t]);
-        sandwich<N>(Bi, Mt, [&](int t, R v) { accH.g(t) += v - fb * Bi[t]; });
+        sandwich_seeded<N>(Bi, Mt, [&](int t) { return accH.g(t) - fb * Bi[t]; },
+                           [&](int t, R v) { accH.g(t) = v; });
 #pragma unroll
         for (int t = 0; t < tri(N); ++t) W[t] = ovk * (6.0 * b(BL::Nk + t) + W[t]);
-        sandwich<N>(Bi, W, [&](int t, R v) { koH.put(t, v - fk * Bi[t]); });
+        sandwich_seeded<N>(Bi, W, [&](int t) { return -(fk * Bi[t]); }, [&](int t, R v) { koH.put(t, v); });
         // S parts: Bi (-1.5 ov B) Bi = -1.5 ov Bi
 #pragma unroll
         for (int t = 0; t < tri(N); ++t) {
-            accS.g(t) += -(sb * Bi[t]);
+            accS.g(t) = accS.g(t) - sb * Bi[t];
             koS.put(t, -(sk * Bi[t]));
         }
     }
@@ -810,8 +836,8 @@ NECG_HD bool term_fused(const BA &b, const KA &kr, const Consts<N> &cs, R wb, R 
                     t += kr[KL::Ap + sx(i, k)] * Ql[3 * k + c];
                 }
                 const R y = Y[3 * i + c];
-                accH.s(3 * i + c) += ob2 * s - fb2 * y;
-                accS.s(3 * i + c) += -(ob2 * y);
+                accH.s(3 * i + c) = (accH.s(3 * i + c) - fb2 * y) + ob2 * s;
+                accS.s(3 * i + c) = accS.s(3 * i + c) - ob2 * y;
                 koH.put(tri(N) + 1 + 3 * i + c, ok2 * t + fk2 * y);
                 koS.put(tri(N) + 1 + 3 * i + c, ok2 * y);
             }
@@ -832,18 +858,22 @@ NECG_HD bool term_fused(const BA &b, const KA &kr, const Consts<N> &cs, R wb, R 
     for (int i = 0; i < N; ++i)
 #pragma unroll
         for (int j = 0; j <= i; ++j) {
-            R s = Qk[3 * i] * T[3 * j] + T[3 * i] * Qk[3 * j];
+            R s = accH.g(sx(i, j));  // the products fuse into the accumulator
             R t = Ql[3 * i] * Dl[3 * j] + Dl[3 * i] * Ql[3 * j];
             R dd = T[3 * i] * T[3 * j], ee = Dl[3 * i] * Dl[3 * j];
 #pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                s += Qk[3 * i + c] * T[3 * j + c];
+                s += T[3 * i + c] * Qk[3 * j + c];
+            }
+#pragma unroll
             for (int c = 1; c < 3; ++c) {
-                s += Qk[3 * i + c] * T[3 * j + c] + T[3 * i + c] * Qk[3 * j + c];
                 t += Ql[3 * i + c] * Dl[3 * j + c] + Dl[3 * i + c] * Ql[3 * j + c];
                 dd += T[3 * i + c] * T[3 * j + c];
                 ee += Dl[3 * i + c] * Dl[3 * j + c];
             }
-            accH.g(sx(i, j)) += s;
-            accS.g(sx(i, j)) += -(ovb * dd);
+            accH.g(sx(i, j)) = s;
+            accS.g(sx(i, j)) = accS.g(sx(i, j)) - ovb * dd;
             koH.add(sx(i, j), -t);
             koS.add(sx(i, j), -(ovk * ee));
         }
