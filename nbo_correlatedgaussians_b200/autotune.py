@@ -78,7 +78,7 @@ def load_cache() -> dict:
 
 
 def save_cache(cache: dict) -> None:
-    tmp = CACHE + ".tmp"
+    tmp = f"{CACHE}.{os.getpid()}.tmp"  # ranks of one node may save at the same time
     with open(tmp, "w") as fh:
         json.dump(cache, fh, indent=1, sort_keys=True)
     os.replace(tmp, CACHE)
