@@ -160,3 +160,29 @@ def test_driver_newton_cg_and_restart(torch_cuda, tmp_path):
     assert np.array_equal(q.x, res["x_opt"])
     f, _ = Engine(q).outprod(q.x)
     assert abs(f - res["f_opt"]) < TOL_E
+
+
+def test_handle_memory_is_reused(torch_cuda):
+    """Handles take their workspace from the library's stream-ordered pool:
+    creating and destroying many in turn reuses the same blocks (device memory
+    in use grows by about one workspace, not by one per handle), and a handle
+    made after many others still evaluates correctly."""
+    torch = torch_cuda
+    from nbo_correlatedgaussians_b200 import synth
+    from nbo_correlatedgaussians_b200.engine import Engine
+    p = synth.make_problem("LiH", 160, 77)
+    eng = Engine(p)
+    ws = eng.L.necg_workspace_bytes(eng.h)
+    eng.close()
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for _ in range(30):
+        Engine(p).close()
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free0 - free1 < 2 * ws + (64 << 20)
+    eng = Engine(p)
+    f, g = eng.outprod(p.x)
+    fo, go = Oracle.from_problem(p).outprod(p.x, nthreads=16)
+    assert abs(f - fo) < TOL_E and normwise(g, go) < 1e-9
+    eng.close()
