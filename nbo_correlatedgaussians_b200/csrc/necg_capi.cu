@@ -36,6 +36,15 @@ using necg::LaunchArgs;
 
 namespace {
 
+// Status code of the two device status words (flags, first failing pair).
+int status_code(const int st[2], long long *bad_pair) {
+    if (bad_pair) *bad_pair = st[1] == 0x7fffffff ? -1 : (long long)st[1];
+    if (st[0] & 1) return NECG_ERR_NOT_PD;
+    if (st[0] & 2) return NECG_ERR_NONFINITE;
+    if (st[0] & 4) return NECG_ERR_ARG;
+    return NECG_OK;
+}
+
 int cuda_fail(cudaError_t e) {
     if (e == cudaSuccess) return NECG_OK;
     return e == cudaErrorMemoryAllocation ? NECG_ERR_ALLOC : NECG_ERR_CUDA;
@@ -469,6 +478,7 @@ int necg_destroy(necg_handle *h) {
     if (!h) return NECG_ERR_ARG;
     cudaSetDevice(h->device);
     free_all(h);
+    if (h->h_tail) cudaFreeHost(h->h_tail);
     delete h;
     return NECG_OK;
 }
@@ -689,9 +699,16 @@ int necg_outprod_host(necg_handle *h, int K, const double *x_host, double *f_hos
     CK(cudaMemcpyAsync(h->d_x, x_host, len * sizeof(double), cudaMemcpyHostToDevice, st));
     rc = necg_outprod(h, K, h->d_x, h->d_f, h->d_g, nullptr, nullptr, stream);
     if (rc) return rc;
+    // f and the status words land in a pinned buffer, so the stream is waited for once
+    if (!h->h_tail) CK(cudaMallocHost((void **)&h->h_tail, 4 * sizeof(double)));
     CK(cudaMemcpyAsync(g_host, h->d_g, len * sizeof(double), cudaMemcpyDeviceToHost, st));
-    if (f_host) CK(cudaMemcpyAsync(f_host, h->d_f, sizeof(double), cudaMemcpyDeviceToHost, st));
-    return necg_status(h, nullptr);
+    CK(cudaMemcpyAsync(h->h_tail, h->d_f, sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(h->h_tail + 1, h->d_status, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (f_host) *f_host = h->h_tail[0];
+    int sw[2];
+    memcpy(sw, h->h_tail + 1, sizeof(sw));
+    return status_code(sw, nullptr);
 }
 
 int necg_make_grad(necg_handle *h, int K, const double *iv_dev, const double *C_dev,
@@ -818,11 +835,7 @@ int necg_status(necg_handle *h, long long *bad_pair) {
     int st[2];
     CK(cudaMemcpyAsync(st, h->d_status, sizeof(st), cudaMemcpyDeviceToHost, h->last_stream));
     CK(cudaStreamSynchronize(h->last_stream));
-    if (bad_pair) *bad_pair = st[1] == 0x7fffffff ? -1 : (long long)st[1];
-    if (st[0] & 1) return NECG_ERR_NOT_PD;
-    if (st[0] & 2) return NECG_ERR_NONFINITE;
-    if (st[0] & 4) return NECG_ERR_ARG;
-    return NECG_OK;
+    return status_code(st, bad_pair);
 }
 
 int necg_profile(necg_handle *h, int enable) {

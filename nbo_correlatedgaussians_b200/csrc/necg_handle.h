@@ -47,6 +47,8 @@ struct necg_handle {
     int npc = 1;
     double *d_Hp = nullptr, *d_Sp = nullptr;  // npc K x K sums each
     size_t hp_cap = 0;                        // doubles per buffer
+    // pinned host landing area of the host entry point: f, then the two status words
+    double *h_tail = nullptr;
 };
 
 namespace necg {
