@@ -101,6 +101,29 @@ def test_outprod_vs_oracle(torch_cuda, system, K):
     assert normwise(Pot.cpu().numpy(), Po) < 1e-12
 
 
+@pytest.mark.parametrize("system", ["He", "H2", "LiH"])
+def test_edge_sizes_every_pass(torch_cuda, system):
+    """One basis function, two, and the sizes either side of a 32-row block, in a
+    handle made for a larger K_max: every pair pass (ordered, symmetric, fused
+    with one-warp tiles, split terms and lockstep blocks) against the oracle."""
+    from nbo_correlatedgaussians_b200 import _lib, synth
+    from nbo_correlatedgaussians_b200.engine import Engine
+    for K in (1, 2, 31, 32, 33):
+        p = synth.make_problem(system, K, 900 + K)
+        p.C = np.random.default_rng(K).normal(size=K)
+        fo, go = Oracle.from_problem(p).outprod(p.x, nthreads=8)
+        eng = Engine(p, K_max=40)
+        L = eng.L
+        for mode, lc, minw, npc in [(0, 4, 8, 1), (1, 2, 8, 1), (2, 2, 118, 1), (2, 1, 118, p.nst),
+                                    (2, 2, 228, 1)]:
+            assert L.necg_set_symmetric(eng.h, mode, lc, minw) == _lib.NECG_OK
+            assert L.necg_set_splits(eng.h, npc) == _lib.NECG_OK
+            f, g = eng.outprod(p.x)
+            assert abs(f - fo) < TOL_E, (K, mode, minw, npc)
+            assert normwise(g, go) < TOL_G, (K, mode, minw, npc)
+        eng.close()
+
+
 def test_make_grad_matches_outprod_gradient(torch_cuda):
     from nbo_correlatedgaussians_b200 import synth
     p = synth.make_problem("H2", 48, 7)
