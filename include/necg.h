@@ -250,8 +250,10 @@ int necg_batch_status_async(necg_batch *b, int *flags_host, void *stream);
  * A problem whose intermediates do not fit the 32 MiB returns
  * NECG_ERR_CAPACITY: K <= 779 for n = 5, nst = 24 (LiH); K <= 1143 for n = 3,
  * nst = 4 (H2); K <= 1247 for n = 2, nst = 2 (He).  The first call on a device looks up the array's device address and
- * must come before any stream capture on that device.  Calls share the array,
- * so calls that overlap on the GPU race; callers serialise them.  No counterpart
+ * must come before any stream capture on that device; the address is kept
+ * for the life of the process, so no call may follow a cudaDeviceReset.  Calls
+ * share the array, so calls that overlap on the GPU race; callers serialise
+ * them.  No counterpart
  * in the reference: its outprod (python/outprod.py:20) allocates as NumPy does. */
 int necg_outprod_noalloc(int n, int nst, int K, double efs, const double *mass_host,
                          const double *ncv_host, const double *scvv_host, const double *sml_host,

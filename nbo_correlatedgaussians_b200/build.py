@@ -1,6 +1,7 @@
 """Build libnecg_b200.so in-tree with nvcc for sm_100a.
 
-The library is plain CUDA C++ behind the C ABI of include/necg.h; it links the
+The library is plain CUDA C++ behind the C ABI of include/necg.h, compiled one
+object per source file (in parallel, under _build/) and linked with the
 CUDA runtime statically so that it does not depend on which libcudart the
 Python process has already loaded.
 """
@@ -10,6 +11,7 @@ import os
 import shutil
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
@@ -19,8 +21,9 @@ HEADERS = ["necg_math.cuh", "necg_kernels.cuh", "necg_lanes.cuh", "necg_handle.h
            "necg_device.cuh", "necg_trace.h"]
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--shared", "-cudart", "static",
-         "-Xptxas", "-v"]
+COMPILE_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xptxas", "-v"]
+LINK_FLAGS = ["-Xcompiler", "-fPIC", "--shared", "-cudart", "static"]
+OBJDIR = os.path.join(os.path.dirname(HERE), "_build")
 
 
 def _nvcc() -> str:
@@ -38,19 +41,34 @@ def _stale() -> bool:
     return any(os.path.getmtime(d) > t for d in deps)
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
-    """Compile the library if it is missing or older than its sources."""
-    if not force and not _stale():
-        return LIB
-    cmd = [_nvcc(), *ARCH, *FLAGS, "-I", INCLUDE, *[os.path.join(CSRC, s) for s in SOURCES], "-o", LIB + ".tmp"]
+def _compile(nvcc: str, src: str, obj: str) -> str:
+    cmd = [nvcc, *ARCH, *COMPILE_FLAGS, "-I", INCLUDE, "-c", os.path.join(CSRC, src), "-o", obj]
     res = subprocess.run(cmd, capture_output=True, text=True)
     if res.returncode != 0:
-        raise RuntimeError("nvcc failed:\n" + res.stdout + res.stderr)
+        raise RuntimeError(f"nvcc failed on {src}:\n" + res.stdout + res.stderr)
+    return res.stderr
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    """Compile the library if it is missing or older than its sources: one nvcc
+    per source file in parallel, then one link."""
+    if not force and not _stale():
+        return LIB
+    nvcc = _nvcc()
+    os.makedirs(OBJDIR, exist_ok=True)
+    objs = [os.path.join(OBJDIR, os.path.splitext(s)[0] + ".o") for s in SOURCES]
+    with ThreadPoolExecutor(max_workers=len(SOURCES)) as ex:
+        reports = list(ex.map(lambda so: _compile(nvcc, *so), zip(SOURCES, objs)))
+    cmd = [nvcc, *ARCH, *LINK_FLAGS, *objs, "-o", LIB + ".tmp"]
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        raise RuntimeError("nvcc link failed:\n" + res.stdout + res.stderr)
     os.replace(LIB + ".tmp", LIB)
+    report = "".join(reports)
     with open(os.path.join(HERE, "ptxas_report.txt"), "w") as fh:
-        fh.write(res.stderr)
+        fh.write(report)
     if verbose:
-        print(res.stderr, file=sys.stderr)
+        print(report, file=sys.stderr)
     return LIB
 
 

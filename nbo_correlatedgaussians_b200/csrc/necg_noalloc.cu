@@ -16,7 +16,10 @@
 // loads this library, held until the process exits.  Every call uses the same
 // array and leaves its contents behind; whatever must start at zero is cleared
 // by the call itself.  Two calls that overlap on the GPU (different streams or
-// host threads) race on the array; callers serialise them.
+// host threads) race on the array; callers serialise them.  The array's device
+// address is looked up once per device and kept for the life of the process, so
+// a cudaDeviceReset (which unloads the library's module) must not be followed
+// by further calls of this entry point.
 #include <cuda_runtime.h>
 #include <string.h>
 
@@ -107,7 +110,7 @@ extern "C" int necg_outprod_noalloc(int n, int nst, int K, double efs, const dou
                                     const double *x_dev, double *f_dev, double *g_dev, void *stream) {
     if (n < 1 || n > 6) return NECG_ERR_UNSUPPORTED;
     if (nst < 1 || K < 1 || !mass_host || !ncv_host || !scvv_host || !sml_host || !sms_host || !x_dev ||
-        !g_dev)
+        !f_dev || !g_dev)
         return NECG_ERR_ARG;
     const Carve c = carve(n, nst, K);
     if (c.total * sizeof(double) > NECG_NOALLOC_SCRATCH_BYTES) return NECG_ERR_CAPACITY;
@@ -156,10 +159,9 @@ extern "C" int necg_outprod_noalloc(int n, int nst, int K, double efs, const dou
     a.g = g_dev;
     a.status = status;
     a.lam = 1.0;
-    if (necg::launch_prep(a, st)) return NECG_ERR_UNSUPPORTED;
-    necg::launch_energy(a, st);
+    if (necg::launch_prep(a, st) || necg::launch_energy(a, st)) return NECG_ERR_UNSUPPORTED;
     necg::launch_rows_finalize(a, f_dev, g_dev + siv, 0, 0.0, 0.0, st);
-    necg::launch_grad(a, st);
+    if (necg::launch_grad(a, st)) return NECG_ERR_UNSUPPORTED;
     if (cudaGetLastError() != cudaSuccess) return NECG_ERR_CUDA;
     // synchronous: report the pair status of this evaluation
     int hs[2] = {0, 0};

@@ -24,3 +24,11 @@ def pytest_collection_modifyitems(config, items):
     for item in items:
         if "gpu" in item.keywords:
             item.add_marker(skip)
+
+
+@pytest.fixture(autouse=True)
+def _biout_into_tmp(tmp_path, monkeypatch):
+    """utils.biout appends to necg.out in the working directory, as the
+    reference's does; point it at the test's own temporary directory."""
+    from nbo_correlatedgaussians_b200 import utils
+    monkeypatch.setattr(utils, "_OUTPUT_FILE", str(tmp_path / "necg.out"))

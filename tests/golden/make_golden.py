@@ -38,7 +38,9 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, REPO)
-REF = os.environ.get("NECG_REF", "/root/reference")
+REF = os.environ.get("NECG_REF")
+if not REF:
+    sys.exit("set NECG_REF to a checkout of MauricioCafiero/NBO_CorrelatedGaussians")
 sys.path.insert(0, os.path.join(REF, "python"))
 
 import shared as sh  # noqa: E402  (reference module)
