@@ -90,8 +90,13 @@ int necg_set_variant(necg_handle *h, int minw_energy, int minw_grad);
  * 122 (the same with each warp's ket record staged in shared memory), 208
  * (as 108, with the 8 warps of an SM in one block stepping through their terms
  * together), 218 (as 208, with the block's bra records staged in shared
- * memory), 228 (as 218, each warp's current ket record staged too), 222 and 232
- * (218 and 228 with 12 warps per block; NECG_ERR_UNSUPPORTED where their shared
+ * memory), 228 (as 218, each warp's ket records staged too, the next one
+ * copied while the current term runs), 248 (as 228 without the barrier after
+ * every term), 258 and 268 (as 228, with warps 4-7 taking their per-term
+ * barrier inside the term -- after the pair's Cholesky factor, inverse and
+ * overlap for 258, after the kinetic and field terms for 268 -- so the two
+ * warps of each scheduler run different parts of the term), 222 and 232 (218
+ * and 228 with 12 warps per block; NECG_ERR_UNSUPPORTED where their shared
  * memory does not fit, n = 5).  Set by the autotuner. */
 int necg_set_symmetric(necg_handle *h, int mode, int lc, int minw);
 

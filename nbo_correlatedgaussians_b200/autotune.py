@@ -40,16 +40,18 @@ LC_E = (2, 4, 8, 16, 32)
 LC_G = (4, 8, 16, 32, 64)
 MINB = (8, 12, 16, 20)
 MINB_GRAD_EXTRA = (112, 116)  # gradient kernel with shared-memory accumulators
-LC_S = (2, 4, 8, 16)          # kets per tile of the symmetric gradient pass
+LC_S = (1, 2, 4, 8, 16)       # kets per tile of the symmetric gradient pass
 MINW_SYM = (8, 12)
-MINW_FUSED = (8, 12, 16, 108, 112, 118, 122, 208, 218, 228, 222, 232)
+MINW_FUSED = (8, 12, 16, 108, 112, 118, 122, 208, 218, 228, 222, 232, 248, 258, 268)
 SPLITS = (1, 2, 3, 4, 6, 8, 12, 24)
 SPLIT_TILES = 2048  # try splits below this many fused tiles
 # 100 + w: ket records re-read at each use (118 / 122: staged in shared memory,
 # 8 / 12 warps); 2xy: lockstep blocks (208 8 warps,
-# 218 + bras in shared memory, 228 + ket record in shared memory, 222 / 232 the
-# same with 12 warps); a variant whose shared memory does not fit for n is refused
-# by necg_set_symmetric and skipped
+# 218 + bras in shared memory, 228 + ket records in shared memory, 248 as 228
+# without a barrier per term, 258 / 268 as 228 with half the warps taking their
+# per-term barrier inside the term, 222 / 232 as 218 / 228 with 12 warps); a
+# variant whose shared memory does not fit for n is refused by
+# necg_set_symmetric and skipped
 
 
 def fused_tiles(K: int, lc: int) -> int:

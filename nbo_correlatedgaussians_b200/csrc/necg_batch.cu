@@ -199,10 +199,10 @@ __global__ void __launch_bounds__(32, 8) batch_fused_warp_kernel(PlanPtrs p) {
 // tiles first) and over each instance's groups (one 32-row block, 8 consecutive
 // ket chunks, one per warp).  The warps of a block work on the same instance and
 // bras and step through their terms together; the group's bras are staged in
-// shared memory once, each warp's current ket record too (fsym_tile with
-// BSYNC, SBRA, SKET).  Shared memory is sized for n = kMaxN.
+// shared memory once, each warp's ket records too, in two buffers (fsym_tile
+// with BSYNC, SBRA, SKET).  Shared memory is sized for n = kMaxN.
 template <int N> __host__ __device__ constexpr int bfused_warp_smem() {
-    return 2 * Part<N>::size * 32 + 2 * 16 * 33 + 32 + KetLayout<N>::size;
+    return 2 * Part<N>::size * 32 + 2 * 16 * 33 + 32 + 2 * KetLayout<N>::size;
 }
 constexpr int kBatchFusedSmem = (8 * bfused_warp_smem<kMaxN>() + BraLayout<kMaxN>::size * 32) * 8;
 
@@ -232,7 +232,7 @@ __device__ __forceinline__ void batch_fused_group(const InstDesc &d, int2 gr, do
 }
 
 __global__ void __launch_bounds__(256, 1) batch_fused_kernel(PlanPtrs p) {
-    extern __shared__ double smem[];
+    extern __shared__ __align__(16) double smem[];
     __shared__ int gsh;
     const int nf = p.hdr->nf, ninst = p.hdr->ninst;
     for (;;) {

@@ -494,7 +494,8 @@ int necg_set_tiles(necg_handle *h, int lc_energy, int lc_grad) {
 }
 
 int necg_set_symmetric(necg_handle *h, int mode, int lc, int minw) {
-    const bool blockv = minw == 208 || minw == 218 || minw == 228 || minw == 222 || minw == 232;
+    const bool blockv = minw == 208 || minw == 218 || minw == 228 || minw == 222 || minw == 232 || minw == 248 ||
+                        minw == 258 || minw == 268;
     const bool okw = minw == 8 || minw == 12 || minw == 16 ||
                      (mode == 2 && (minw == 108 || minw == 112 || minw == 118 || minw == 122 || blockv));
     if (!h || mode < 0 || mode > 2 || lc < 1 || lc > 64 || !okw) return NECG_ERR_ARG;

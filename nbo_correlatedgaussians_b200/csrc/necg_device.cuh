@@ -23,6 +23,28 @@ template <int N> struct SmemAcc {
     __device__ __forceinline__ double &s(int t) { return p[(tri(N) + 1 + t) * 32]; }
 };
 
+// Block barrier that warps may reach from different places in the code (the
+// non-aligned form of bar.sync: __syncthreads requires every thread of the
+// block to execute the same barrier instruction).  Every warp of the block
+// must still call it the same number of times.
+__device__ __forceinline__ void cta_barrier() { asm volatile("barrier.sync 0;" ::: "memory"); }
+
+// Copy a ket record of nd doubles (nd even: records are 16-byte multiples, at
+// 16-byte aligned addresses) from global to shared memory without waiting:
+// 16-byte cp.async per lane, one commit group per record.
+__device__ __forceinline__ void ket_fetch(double *dst, const double *src, int nd, int lane) {
+    for (int i = lane; 2 * i < nd; i += 32) {
+        const unsigned d = (unsigned)__cvta_generic_to_shared(dst + 2 * i);
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src + 2 * i) : "memory");
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
+// Wait for this lane's copies and make the warp's copies visible to the warp.
+__device__ __forceinline__ void ket_wait() {
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    __syncwarp();
+}
+
 // Status word: [0] bit flags, [1] first failing pair (row-major k*K + l).
 __device__ __forceinline__ void flag_status(int *status, int flags, int pair) {
     if (!flags) return;
@@ -35,7 +57,7 @@ __device__ __forceinline__ void flag_status(int *status, int flags, int pair) {
 // reduction row (32).  Sized by the caller for its largest n.
 struct FusedSmem {
     double *sacc, *krow, *kred;
-    double *sket;  // SKET: this warp's copy of the current ket record
+    double *sket;  // SKET: two ket-record buffers of this warp (16-byte aligned)
 };
 
 // One tile of the fused pass over unordered pairs (k >= l): the symmetric
@@ -61,12 +83,18 @@ struct FusedSmem {
 // SBRA: the block's 32 bras of row block tl.x are staged in shared memory at
 // sbra (field f of lane j at sbra[f * 32 + j]; rows past K hold row K - 1) and
 // read there instead of from global memory.
-// SKET: each (l, P) ket record is copied by the warp into sm.sket and read
-// there.
+// SKET: each (l, P) ket record is copied by the warp into one of its two
+// buffers at sm.sket and read there; the copy of the next term's record
+// (cp.async) runs while the current term is evaluated.
 // [p0, p1): the symmetry terms this tile takes (p1 < 0: all nst).  A pass whose
 // tiles split the terms writes each split's partials to its own slot (t is then
 // the slot index) and each split's H, S sums to its own K x K buffer.
-template <int N, bool VKET, bool BSYNC = false, bool SBRA = false, bool SKET = false>
+// SYNC (with BSYNC): 0 -- every warp takes the block barrier at the end of
+// each term; 1, 2 -- warps 4-7 of the block take it inside the term instead
+// (at term_fused's mid(1): after B, Bi, T and ov; mid(2): after tau and sig),
+// so the two warps of each scheduler run different stretches of the body; 3 --
+// no barrier per term (the warps only meet at the tile group's barriers).
+template <int N, bool VKET, bool BSYNC = false, bool SBRA = false, bool SKET = false, int SYNC = 0>
 __device__ __forceinline__ void fsym_tile(int t, int2 tl, int LC, int K, int nst, const Consts<N> &cs,
                                           const double *__restrict__ bra, const double *__restrict__ ket,
                                           const double *__restrict__ C, const KetMap &kmap,
@@ -77,6 +105,9 @@ __device__ __forceinline__ void fsym_tile(int t, int2 tl, int LC, int K, int nst
     using KL = KetLayout<N>;
     constexpr int PS = Part<N>::size;
     static_assert(PS <= 32, "the symmetric pass needs tri(n) + 1 + 3n <= 32");
+    // a barrier inside the term is taken only on the path that passes mid to
+    // term_fused; anywhere else the warps' barrier counts would not match
+    static_assert(SYNC == 0 || SYNC == 3 || (BSYNC && SBRA && SKET), "mid-term barriers need BSYNC, SBRA, SKET");
     const int lane = threadIdx.x & 31;
     double *krow0 = sm.krow, *krow1 = sm.krow + 16 * 33, *kred = sm.kred;
     const int k = tl.x * 32 + lane;
@@ -102,35 +133,61 @@ __device__ __forceinline__ void fsym_tile(int t, int2 tl, int LC, int K, int nst
     } koH{krow0 + (lane >> 1) * 33, !(lane & 1)}, koS{krow1 + (lane >> 1) * 33, !(lane & 1)};
     bool ok = true;
     int flags = 0, bad = 0x7fffffff;  // smallest failing pair (row-major k K + l)
+    // where this warp takes its per-term block barrier (BSYNC): 0 at the end of
+    // the term, 1 / 2 at term_fused's mid(1) / mid(2), -1 nowhere.  Every warp
+    // takes exactly one barrier per (l, P) term, or none (SYNC 3).
+    const int sync_at = !BSYNC || SYNC == 3 ? -1 : SYNC == 0 || !((threadIdx.x >> 7) & 1) ? 0 : SYNC;
+    struct MidSync {
+        int at;
+        __device__ __forceinline__ void operator()(int i) const {
+            if (i == at) cta_barrier();
+        }
+    } mid{sync_at};
+    const int pend = p1 < 0 ? nst : p1;
+    // warp-uniform: ket l has work (always, without BSYNC); false from the
+    // first l without work to the end of the tile
+    auto has_work = [&](int l) { return !BSYNC || (!idle && l < K); };
+    int cur = 0;  // SKET: the buffer that holds the current term's record
+    if constexpr (SKET) {
+        if (l0 < l1 && p0 < pend && has_work(l0))
+            ket_fetch(sm.sket, ket + ((size_t)l0 * nst + p0) * KL::size, KL::size, lane);
+    }
     for (int l = l0; l < l1; ++l) {
-        // warp-uniform: this (l) has work (always, without BSYNC)
-        const bool lok = !BSYNC || (!idle && l < K);
+        const bool lok = has_work(l);
         double aH = 0.0, aS = 0.0, hsum = 0.0, ssum = 0.0;
         const bool active = kval && l <= k && lok;
         const BraRef b{bra + (active ? k : (lok ? l : 0)), (size_t)K};
-        const int pend = p1 < 0 ? nst : p1;
         for (int P = p0; P < pend; ++P) {
             if (BSYNC && !lok) {
-                __syncthreads();
+                if (sync_at >= 0) cta_barrier();
                 continue;
             }
             const double *kr = ket + ((size_t)l * nst + P) * KL::size;
             if constexpr (SKET) {
-                for (int i = lane; i < KL::size; i += 32) sm.sket[i] = kr[i];
-                __syncwarp();
+                ket_wait();  // this term's record is in buffer cur
+                int nl = l, nP = P + 1;
+                if (nP >= pend) {
+                    nl = l + 1;
+                    nP = p0;
+                }
+                if (nl < l1 && has_work(nl))
+                    ket_fetch(sm.sket + (cur ^ 1) * KL::size, ket + ((size_t)nl * nst + nP) * KL::size, KL::size,
+                              lane);
+                kr = sm.sket + cur * KL::size;
+                cur ^= 1;
             }
             const double wb = active ? kr[KL::wC] : 0.0;
             const double wk = active && l < k ? 2.0 * Ck * kr[KL::winv] : 0.0;
             double h, ov;
             bool tok;
             if constexpr (SBRA && SKET)
-                tok = term_fused<N, double>(BraSmem{sbra + lane}, KetSmem{sm.sket}, cs, wb, wk, accH, accS, koH, koS,
-                                            h, ov);
+                tok = term_fused<N, double>(BraSmem{sbra + lane}, KetSmem{kr}, cs, wb, wk, accH, accS, koH, koS, h,
+                                            ov, mid);
             else if constexpr (SBRA)
                 tok = term_fused<N, double>(BraSmem{sbra + lane}, KetRefV{kr}, cs, wb, wk, accH, accS, koH, koS, h,
-                                            ov);
+                                            ov, mid);
             else if constexpr (SKET)
-                tok = term_fused<N, double>(b, KetSmem{sm.sket}, cs, wb, wk, accH, accS, koH, koS, h, ov);
+                tok = term_fused<N, double>(b, KetSmem{kr}, cs, wb, wk, accH, accS, koH, koS, h, ov);
             else if constexpr (VKET)
                 tok = term_fused<N, double>(b, KetRefV{kr}, cs, wb, wk, accH, accS, koH, koS, h, ov);
             else
@@ -161,7 +218,7 @@ __device__ __forceinline__ void fsym_tile(int t, int2 tl, int LC, int K, int nst
                 }
                 __syncwarp();
             }
-            if (BSYNC) __syncthreads();
+            if (BSYNC && sync_at == 0) cta_barrier();
         }
         if (BSYNC && !lok) continue;
         if (active) {

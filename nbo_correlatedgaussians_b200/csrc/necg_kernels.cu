@@ -289,7 +289,7 @@ __global__ void __launch_bounds__(32, MINW) fsym_kernel(const int2 *__restrict__
     __shared__ double sacc[2 * Part<N>::size * 32];
     __shared__ double krow[2 * 16 * 33];
     __shared__ double kred[32];
-    __shared__ double sket[SKET ? KetLayout<N>::size : 2];
+    __shared__ __align__(16) double sket[SKET ? 2 * KetLayout<N>::size : 2];
     const int t = t_begin + blockIdx.x;
     if (t >= t_end) return;
     const int pc = blockIdx.y, PC = (nst + npc - 1) / npc;
@@ -320,17 +320,19 @@ __global__ void __launch_bounds__(256) hs_reduce_kernel(const double *__restrict
 // - 1, one per warp.  The warps read the same 32 bras and step through their
 // terms together (fsym_tile with BSYNC), so the warps sharing a scheduler run
 // the same stretch of the long term body.  SBRA: the group's bras are staged in
-// shared memory once for all warps; SKET: each warp stages its current ket
-// record.  Shared memory (dynamic): per warp 2 PS 32 + 2 16 33 + 32 (+ the ket
-// record) doubles, then the bras.
+// shared memory once for all warps; SKET: each warp stages its ket records in
+// two buffers (the next term's copied while the current one is evaluated).
+// SYNC: where the warps take their per-term barrier (fsym_tile).  Shared
+// memory (dynamic, 16-byte aligned): per warp 2 PS 32 + 2 16 33 + 32 (+ 2 ket
+// records) doubles, then the bras.
 template <int N> __host__ __device__ constexpr int fsym_warp_smem(bool sket) {
-    return 2 * Part<N>::size * 32 + 2 * 16 * 33 + 32 + (sket ? KetLayout<N>::size : 0);
+    return 2 * Part<N>::size * 32 + 2 * 16 * 33 + 32 + (sket ? 2 * KetLayout<N>::size : 0);
 }
 template <int N> __host__ __device__ constexpr int fsym_block_smem_bytes(int warps, bool sbra, bool sket) {
     return (warps * fsym_warp_smem<N>(sket) + (sbra ? BraLayout<N>::size * 32 : 0)) * 8;
 }
 
-template <int N, bool VKET, bool SBRA, bool SKET, int WARPS>
+template <int N, bool VKET, bool SBRA, bool SKET, int WARPS, int SYNC = 0>
 __global__ void __launch_bounds__(32 * WARPS, 1) fsym_block_kernel(const int2 *__restrict__ groups, int ngroups,
                                                                 int *__restrict__ qcount,
                                                                 const int *__restrict__ tstart, int LC, int K,
@@ -341,7 +343,7 @@ __global__ void __launch_bounds__(32 * WARPS, 1) fsym_block_kernel(const int2 *_
                                                                 double *__restrict__ H, double *__restrict__ S,
                                                                 double *__restrict__ part_b,
                                                                 double *__restrict__ part_k, int *status) {
-    extern __shared__ double smem[];
+    extern __shared__ __align__(16) double smem[];
     __shared__ int gsh;
     constexpr int PS = Part<N>::size;
     constexpr int PER_WARP = fsym_warp_smem<N>(SKET);
@@ -368,8 +370,8 @@ __global__ void __launch_bounds__(32 * WARPS, 1) fsym_block_kernel(const int2 *_
             }
             __syncthreads();
         }
-        fsym_tile<N, VKET, true, SBRA, SKET>(tstart[kb] + lc, make_int2(kb, lc), LC, K, nst, cs, bra, ket, C, kmap,
-                                             H, S, part_b, part_k, status, sm, idle, sbra);
+        fsym_tile<N, VKET, true, SBRA, SKET, SYNC>(tstart[kb] + lc, make_int2(kb, lc), LC, K, nst, cs, bra, ket, C,
+                                                   kmap, H, S, part_b, part_k, status, sm, idle, sbra);
         if constexpr (SBRA) __syncthreads();  // sbra is rewritten for the next group
     }
 }
@@ -765,11 +767,12 @@ template <int N> struct Launch {
                 npc > 1 ? a.Sp : a.S, a.psym, a.psym + (size_t)a.nstiles * npc * 2 * Part<N>::size * 32, a.status);
         }
     }
-    template <bool SBRA, bool SKET, int WARPS> static void fsym_block(const LaunchArgs &a, cudaStream_t st) {
+    template <bool SBRA, bool SKET, int WARPS, int SYNC = 0>
+    static void fsym_block(const LaunchArgs &a, cudaStream_t st) {
         if constexpr (Part<N>::size <= 32) {
             constexpr int smem = fsym_block_smem_bytes<N>(WARPS, SBRA, SKET);
             if constexpr (smem <= 232448) {
-                auto kern = fsym_block_kernel<N, true, SBRA, SKET, WARPS>;
+                auto kern = fsym_block_kernel<N, true, SBRA, SKET, WARPS, SYNC>;
                 int dev = 0, sms = 148;
                 cudaGetDevice(&dev);
                 // the shared-memory opt-in is per device: once per instantiation and device
@@ -794,6 +797,9 @@ template <int N> struct Launch {
             switch (a.minb_s) {  // 2xy: lockstep blocks; see fused_variant_ok
             case 218: fsym_block<true, false, 8>(a, st); break;
             case 228: fsym_block<true, true, 8>(a, st); break;
+            case 248: fsym_block<true, true, 8, 3>(a, st); break;
+            case 258: fsym_block<true, true, 8, 1>(a, st); break;
+            case 268: fsym_block<true, true, 8, 2>(a, st); break;
             case 222: fsym_block<true, false, 12>(a, st); break;
             case 232: fsym_block<true, true, 12>(a, st); break;
             default: fsym_block<false, false, 8>(a, st); break;
@@ -896,7 +902,8 @@ int fused_block_warps(int variant) { return variant == 222 || variant == 232 ? 1
 bool fused_variant_ok(int n, int variant) {
     if (variant < 200) return true;
     if (n < 1 || n > 5) return false;
-    const bool sbra = variant != 208, sket = variant == 228 || variant == 232;
+    const bool sbra = variant != 208,
+               sket = variant == 228 || variant == 232 || variant == 248 || variant == 258 || variant == 268;
     const int warps = fused_block_warps(variant);
     int bytes = 0;
     switch (n) {

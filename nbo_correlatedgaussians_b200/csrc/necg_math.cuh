@@ -179,6 +179,25 @@ template <int N, typename R> struct RegAcc {
 };
 
 // ---------------------------------------------------------------------------
+// x^(-1/2) for normal, positive x.  On the device the hardware approximation
+// rsqrt.approx.ftz.f64 (relative error below 1e-6) is refined by one step of
+// Householder's third-order iteration for 1/sqrt(x): with r = 1 - x y^2,
+// y <- y + y r (1/2 + 3/8 r), the series of (1 - r)^(-1/2) to second order,
+// whose truncation error (of order r^3) lies far below the result's rounding.
+// Measured on a B200 over 2^24 inputs in [2^-40, 2^40]: within 2 ulp of
+// rsqrt(double) and 2.4 ulp of 1 / sqrt(x), at 1.56x its throughput.  Host
+// builds (the emulator) use 1 / sqrt(x).
+NECG_HD double rsq(double x) {
+#ifdef __CUDA_ARCH__
+    double y;
+    asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+    const double r = fma(-(x * y), y, 1.0);
+    return fma(y * r, fma(0.375, r, 0.5), y);
+#else
+    return 1.0 / ::sqrt(x);
+#endif
+}
+
 // Cholesky of a packed SPD matrix B = R R^T; returns the inverse Bi (packed),
 // prod(1/R_ii) and a success flag.  Fully unrolled into registers.
 #pragma nv_exec_check_disable
@@ -195,7 +214,7 @@ NECG_HD bool chol_inverse(const R (&B)[tri(N)], R (&Bi)[tri(N)], R &prod_rinv) {
         const bool pos = d > 0.0;
         ok = ok && pos;
         if (!pos) d = R(1.0);
-        const R r = rsqrt(d);
+        const R r = rsq(d);
         rinv[j] = r;
         Rm[sx(j, j)] = d * r;
 #pragma unroll
@@ -239,15 +258,22 @@ NECG_HD bool chol_inverse(const R (&B)[tri(N)], R (&Bi)[tri(N)], R &prod_rinv) {
 #pragma nv_exec_check_disable
 template <int N, typename R, typename Acc>
 NECG_HD void symv3(const Acc &S, int off, const R (&x)[3 * N], R (&y)[3 * N]) {
+    // each element of S is read once and used for the three columns (the
+    // accessors may load from memory at every call)
 #pragma unroll
-    for (int i = 0; i < N; ++i)
+    for (int i = 0; i < N; ++i) {
+        {
+            const R a = S[off + sx(i, 0)];
 #pragma unroll
-        for (int c = 0; c < 3; ++c) {
-            R s = S[off + sx(i, 0)] * x[c];
-#pragma unroll
-            for (int k = 1; k < N; ++k) s += S[off + sx(i, k)] * x[3 * k + c];
-            y[3 * i + c] = s;
+            for (int c = 0; c < 3; ++c) y[3 * i + c] = a * x[c];
         }
+#pragma unroll
+        for (int k = 1; k < N; ++k) {
+            const R a = S[off + sx(i, k)];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) y[3 * i + c] += a * x[3 * k + c];
+        }
+    }
 }
 
 // Boys-function pieces for one Coulomb pair.  Given a = v^T Bi v and
@@ -264,7 +290,7 @@ NECG_HD void symv3(const Acc &S, int off, const R (&x)[3 * N], R (&y)[3 * N]) {
 #pragma nv_exec_check_disable
 template <bool GRAD, typename R>
 NECG_HD void boys(R a, R bb, R &fs, R &dfs, R &ia, R &z) {
-    const R ra = rsqrt(a);
+    const R ra = rsq(a);
     ia = ra * ra;
     z = bb * ia;
     if (z <= NECG_F0_SPLIT) {
@@ -272,7 +298,7 @@ NECG_HD void boys(R a, R bb, R &fs, R &dfs, R &ia, R &z) {
                        NECG_PC5) * z + 1.0;
         const R den = (((((NECG_PC6 * z + NECG_PC7) * z + NECG_PC8) * z + NECG_PC9) * z +
                         NECG_PC10) * z + NECG_PC11) * z + 1.0;
-        const R q = rsqrt(num * den);
+        const R q = rsq(num * den);
         const R F0 = num * q;
         fs = F0 * ra;
         if (GRAD) {
@@ -286,7 +312,7 @@ NECG_HD void boys(R a, R bb, R &fs, R &dfs, R &ia, R &z) {
         }
     } else {
         // F0 = sqrt(pi / (4 z)) ; F0 a^-1/2 = sqrt(pi / (4 bb))
-        const R rb = rsqrt(bb);
+        const R rb = rsq(bb);
         fs = (0.5 * NECG_SQRT_PI) * rb;
         if (GRAD) dfs = -0.5 * fs * a * rb * rb;  // F0' = -F0 / (2 z)
         else dfs = R(0.0);
@@ -747,16 +773,23 @@ NECG_HD bool term_sym(const BA &b, const KA &kr, const Consts<N> &cs, R E, R wb,
 //   bra, H: the formulas of term_grad with Fw = Fb, ovw = ovb
 //   bra, S: d(ov)/dA_k = ov (-Dk Dk^T - 1.5 Bi + 0.75 A_k^-1), d(ov)/ds_k = -2 ov Y
 // and the ket formulas of term_sym with the same split (koH, koS).
+// mid(i) is called at two points of the body (i = 1 after B, Bi, T and ov;
+// i = 2 after tau and sig), for callers that synchronise warps there.
+struct NoMid {
+    NECG_HD void operator()(int) const {}
+};
 #pragma nv_exec_check_disable
-template <int N, typename R, typename BA, typename KA, typename ACC, typename KOUT>
+template <int N, typename R, typename BA, typename KA, typename ACC, typename KOUT, typename MID = NoMid>
 NECG_HD bool term_fused(const BA &b, const KA &kr, const Consts<N> &cs, R wb, R wk, ACC &accH, ACC &accS,
-                        KOUT &koH, KOUT &koS, R &h_out, R &ov_out) {
+                        KOUT &koH, KOUT &koS, R &h_out, R &ov_out, const MID &mid = MID{}) {
     using KL = KetLayout<N>;
     using BL = BraLayout<N>;
     R Bi[tri(N)], T[3 * N], ov;
     const bool ok = term_core<N>(b, kr, cs, Bi, T, ov);
+    mid(1);
     const R tau = term_tau<N>(b, kr, cs, Bi, T);
     const R sig = term_sig<N>(cs, T);
+    mid(2);
     R Z[3 * N], W[tri(N)], rho;
     coulomb_grad<N>(Bi, T, cs, rho, Z, W);
     const R h = ov * (2.0 * tau + rho - sig);
@@ -793,15 +826,25 @@ NECG_HD bool term_fused(const BA &b, const KA &kr, const Consts<N> &cs, R wb, R 
 #pragma unroll
     for (int t = 0; t < 3 * N; ++t) Dl[t] = T[t] - kr[KL::Sp + t];
     symv3<N>(kr, KL::Ap, Dl, Y);
+    // the ket and bra matrices below are read once per element and used for
+    // the three columns; each output's products are summed in the same order
 #pragma unroll
-    for (int i = 0; i < N; ++i)
+    for (int i = 0; i < N; ++i) {
+        R s[3];
+        {
+            const R a = kr[KL::AMp + i * N];
 #pragma unroll
-        for (int c = 0; c < 3; ++c) {
-            R s = kr[KL::AMp + i * N] * Y[c];
-#pragma unroll
-            for (int k = 1; k < N; ++k) s += kr[KL::AMp + i * N + k] * Y[3 * k + c];
-            Z[3 * i + c] -= 4.0 * s;
+            for (int c = 0; c < 3; ++c) s[c] = a * Y[c];
         }
+#pragma unroll
+        for (int k = 1; k < N; ++k) {
+            const R a = kr[KL::AMp + i * N + k];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) s[c] += a * Y[3 * k + c];
+        }
+#pragma unroll
+        for (int c = 0; c < 3; ++c) Z[3 * i + c] -= 4.0 * s[c];
+    }
     R Qk[3 * N], Ql[3 * N];
 #pragma unroll
     for (int i = 0; i < N; ++i)
@@ -825,22 +868,34 @@ NECG_HD bool term_fused(const BA &b, const KA &kr, const Consts<N> &cs, R wb, R 
     {
         const R ob2 = 2.0 * ovb, fb2 = 2.0 * Fb, ok2 = 2.0 * ovk, fk2 = 2.0 * Fk;
 #pragma unroll
-        for (int i = 0; i < N; ++i)
+        for (int i = 0; i < N; ++i) {
+            R s[3], t[3];
+            {
+                const R a = b(BL::A + sx(i, 0)), ap = kr[KL::Ap + sx(i, 0)];
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    s[c] = a * Qk[c];
+                    t[c] = ap * Ql[c];
+                }
+            }
+#pragma unroll
+            for (int k = 1; k < N; ++k) {
+                const R a = b(BL::A + sx(i, k)), ap = kr[KL::Ap + sx(i, k)];
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    s[c] += a * Qk[3 * k + c];
+                    t[c] += ap * Ql[3 * k + c];
+                }
+            }
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
-                R s = b(BL::A + sx(i, 0)) * Qk[c];
-                R t = kr[KL::Ap + sx(i, 0)] * Ql[c];
-#pragma unroll
-                for (int k = 1; k < N; ++k) {
-                    s += b(BL::A + sx(i, k)) * Qk[3 * k + c];
-                    t += kr[KL::Ap + sx(i, k)] * Ql[3 * k + c];
-                }
                 const R y = Y[3 * i + c];
-                accH.s(3 * i + c) = (accH.s(3 * i + c) - fb2 * y) + ob2 * s;
+                accH.s(3 * i + c) = (accH.s(3 * i + c) - fb2 * y) + ob2 * s[c];
                 accS.s(3 * i + c) = accS.s(3 * i + c) - ob2 * y;
-                koH.put(tri(N) + 1 + 3 * i + c, ok2 * t + fk2 * y);
+                koH.put(tri(N) + 1 + 3 * i + c, ok2 * t[c] + fk2 * y);
                 koS.put(tri(N) + 1 + 3 * i + c, ok2 * y);
             }
+        }
     }
     // H: Rk = ovb Qk - Fb/2 Dk, acc += Rk Dk^T + Dk Rk^T ; Rl = ovk Ql + Fk/2 Dl, ket -= Rl Dl^T + Dl Rl^T
     // S: bra -= ovb Dk Dk^T, ket -= ovk Dl Dl^T

@@ -22,9 +22,10 @@ def build() -> str:
     if os.path.exists(LIB) and all(os.path.getmtime(LIB) >= os.path.getmtime(d) for d in deps):
         return LIB
     nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    tmp = f"{LIB}.{os.getpid()}.tmp"  # processes started together may build at the same time
     subprocess.check_call([nvcc, "-O1", "-std=c++17", "-Xcompiler", "-fPIC", "--shared",
-                           "-Wno-deprecated-gpu-targets", "-o", LIB + ".tmp", SRC])
-    os.replace(LIB + ".tmp", LIB)
+                           "-Wno-deprecated-gpu-targets", "-o", tmp, SRC])
+    os.replace(tmp, LIB)
     return LIB
 
 

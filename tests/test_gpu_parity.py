@@ -115,7 +115,7 @@ def test_edge_sizes_every_pass(torch_cuda, system):
         eng = Engine(p, K_max=40)
         L = eng.L
         for mode, lc, minw, npc in [(0, 4, 8, 1), (1, 2, 8, 1), (2, 2, 118, 1), (2, 1, 118, p.nst),
-                                    (2, 2, 228, 1)]:
+                                    (2, 2, 228, 1), (2, 1, 248, 1), (2, 2, 258, 1), (2, 1, 268, 1)]:
             assert L.necg_set_symmetric(eng.h, mode, lc, minw) == _lib.NECG_OK
             assert L.necg_set_splits(eng.h, npc) == _lib.NECG_OK
             f, g = eng.outprod(p.x)
@@ -255,7 +255,7 @@ def test_fused_pass_matches_oracle(torch_cuda, system, K, lc):
     assert L.necg_set_symmetric(eng.h, 1, lc, 8) == _lib.NECG_OK
     f1, g1 = eng.outprod(p.x)
     fr, gr, Hr, Sr = Oracle.from_problem(p).outprod(p.x, nthreads=8, return_hs=True)
-    for minw in (8, 12, 16, 108, 112, 118, 122, 208, 218, 228, 222, 232):
+    for minw in (8, 12, 16, 108, 112, 118, 122, 208, 218, 228, 222, 232, 248, 258, 268):
         rc = L.necg_set_symmetric(eng.h, 2, lc, minw)
         if rc == _lib.NECG_ERR_UNSUPPORTED and minw in (222, 232) and p.n == 5:
             continue  # 12 warps of n = 5 do not fit in shared memory
@@ -328,7 +328,7 @@ def test_fused_pass_split_terms(torch_cuda, system, K, lc):
     assert abs(f4 - fr) < TOL_E and normwise(g4, gr) < TOL_G
 
 
-@pytest.mark.parametrize("minw", [8, 118, 208, 228])
+@pytest.mark.parametrize("minw", [8, 118, 208, 228, 248, 258, 268])
 def test_fused_pass_oldquit_and_errors(torch_cuda, minw):
     """The fused mode on the reference's input file, and the pair-status path
     (a singular A_k + A_l') leaving the handle usable, for one-warp and lockstep
