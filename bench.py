@@ -17,7 +17,15 @@ K*30 + K parameters) of the seeded synthetic LiH K=1024 basis.
   CUDA-event duration, against the FP64 FMA throughput measured on this GPU.
 * cpu_baseline: the oracle (a C restatement of the reference's matel/gradel
   loops) on all host cores over a random sample of the workload's terms,
-  extrapolated to evals/s.
+  extrapolated to evals/s; beside it, the reference Python's own outprod as
+  timed by oracle/time_reference.py where a checkout of the reference exists
+  (it has no packaging and cannot travel to this machine).
+* parity: E and g of the timed evaluation against the oracle's full-size
+  fixture (tests/golden/fullsize_<workload>.npz), checked after the timed
+  region.
+* dropin: evals/s through the drop-in module API (outprod.outprod with the
+  shared module state, python/outprod.py:20), with and without copying H and
+  S back, host wall clock.
 * --impl reference: the same CPU port timed as the reference arm.
 Multi-GPU (torchrun): every rank evaluates its own replica of the workload
 (no collective on the data path); value = all ranks' evals / max rank time.
@@ -61,15 +69,66 @@ def parse():
     ap.add_argument("--serve-runs", type=int, default=256,
                     help="truncated-Newton runs (the first of the 256-run serving stream) for the served "
                          "latency / throughput figures; 0 skips them")
-    ap.add_argument("--serve-maxfun", type=int, default=6, help="evaluations per run of that stream")
+    ap.add_argument("--serve-maxfun", type=int, default=50, help="evaluations per run of that stream")
+    ap.add_argument("--no-dropin", action="store_true", help="skip the drop-in module figure")
     ap.add_argument("--serve-procs", type=int, default=-1,
                     help="client processes for the served figures (0: clients as threads of the bench process; "
                          "default: min(12, host cores - 2))")
     return ap.parse_args()
 
 
-DEFAULT_TILES = {"lc_e": 2, "minb_e": 16, "lc_g": 4, "minb_g": 8, "sym": 2, "lc_s": 2, "minw_s": 228}
+DEFAULT_TILES = {"lc_e": 2, "minb_e": 16, "lc_g": 4, "minb_g": 8, "sym": 2, "lc_s": 1, "minw_s": 258}
 PASS_MODE = {"ordered": 0, "symmetric": 1, "fused": 2}
+# FP64 FLOPs per (k, l, P) term (FMA = 2; each div/sqrt/rsqrt/exp = 1), frozen at
+# the counts the kernels' own templates gave when the fused pass was first
+# measured; the roofline fraction is reported at these and at the current count
+FROZEN_FLOPS = {5: {"energy": 1339, "grad": 3337, "sym": 4362, "fused": 4639},
+                3: {"energy": 511, "grad": 1236, "sym": 1586, "fused": 1710},
+                2: {"energy": 253, "grad": 598, "sym": 762, "fused": 832}}
+FIXTURES = {"lih_k1024": "fullsize_lih_k1024.npz", "h2_k2048": "fullsize_h2_k2048.npz"}
+
+
+def bench_config(args, world: int) -> dict:
+    """The workload, as both arms print it."""
+    from nbo_correlatedgaussians_b200 import synth
+    prob = synth.workload(args.workload)
+    K, nst = prob.K, prob.nst
+    return {"workload": args.workload, "desc": WORKLOADS[args.workload],
+            "pair_elements_per_eval": prob.pairs, "terms_per_eval": (prob.pairs + K * K) * nst,
+            "l2": "flushed between steps by a 256 MiB write, not timed",
+            "parallelism": f"replicas x{world}" if world > 1 else "single GPU"}
+
+
+def parity_against_fixture(workload: str, E: float, g) -> dict | None:
+    """|dE| and the norm-wise gradient error against the oracle's full-size
+    fixture (made by tests/golden/make_fullsize.py)."""
+    name = FIXTURES.get(workload)
+    path = os.path.join(HERE, "tests", "golden", name) if name else None
+    if not path or not os.path.exists(path):
+        return None
+    d = np.load(path)
+    dE = abs(E - float(d["f"]))
+    dg = float(np.max(np.abs(g - d["g"])) / np.max(np.abs(d["g"])))
+    return {"fixture": f"tests/golden/{name}", "dE_Eh": dE, "g_normwise": dg, "tol": {"E_Eh": 1e-10, "g": 1e-9},
+            "ok": bool(dE < 1e-10 and dg < 1e-9)}
+
+
+def python_reference_timing() -> dict | None:
+    """The reference Python's own outprod, timed by oracle/time_reference.py
+    where a checkout of the reference exists (not on this machine)."""
+    path = os.path.join(HERE, "oracle", "reference_python_timing.json")
+    if not os.path.exists(path):
+        return None
+    d = json.load(open(path))
+    k12, k1024 = d["lih_k12_all_cores"], d["lih_k1024_extrapolated"]
+    return {"kind": "python", "measured_on": f"{d['host']}, {d['cores']} cores (the build machine, not this one)",
+            "lih_k12_evals_per_s": k12["evals_per_s"],
+            "lih_k12_s_per_eval_one_process": d["lih_k12_one_process"]["s_per_eval"],
+            "lih_k1024_evals_per_s_extrapolated": k1024["evals_per_s_on_all_cores"],
+            "lih_k1024_core_seconds_per_eval": k1024["core_seconds_per_eval"],
+            "why_not_here": "the reference ships no setup.py/pyproject, so it cannot be installed to travel "
+                            "to the GPU machine, and its sources may not be copied into this repository",
+            "source": "oracle/reference_python_timing.json (oracle/time_reference.py)"}
 
 
 # ----------------------------------------------------------------------------- CPU port
@@ -129,12 +188,13 @@ def run_reference(args):
         walls.append(time.perf_counter() - t0)
         rates.append(last["value"])
     value = statistics.mean(rates)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     out = {"metric": METRIC, "value": value, "unit": "evals/s", "impl": "reference", "n_gpus": args.gpus,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * statistics.mean(walls),
            "ms_per_eval_extrapolated": 1e3 / value, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded, oldquit.dat layout)",
-           "config": {"workload": args.workload, "desc": WORKLOADS[args.workload]},
-           "cpu_baseline": dict(last, value=value),
+           "config": bench_config(args, world),
+           "cpu_baseline": dict(last, value=value, python_reference=python_reference_timing()),
            "e2e": {"value": value, "unit": "evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
            "note": "reference arm = oracle/ C port of the reference's matel/gradel loops (the reference "
                    "itself is Python and cannot travel to the GPU box); each step times a bounded random "
@@ -275,6 +335,7 @@ def run_engine(args):
     clk = clocks.stop() if clocks else None
     eng.raise_status("timed steps")
     E = float(f.item())
+    parity = parity_against_fixture(args.workload, E, g.cpu().numpy())
     total = torch.tensor([sum(step_ms)], dtype=torch.float64, device="cuda")
     if world > 1:
         dist.all_reduce(total, op=dist.ReduceOp.MAX)
@@ -313,6 +374,7 @@ def run_engine(args):
 
     K, nst, n = prob.K, prob.nst, prob.n
     tf = term_flops(n)
+    frozen = FROZEN_FLOPS.get(n, {})
     mode = int(tiles.get("sym", 0))
     unordered = (K * (K + 1) // 2) * nst
     ph = np.array(phases)
@@ -332,17 +394,27 @@ def run_engine(args):
         kern_flops, kern_ms = K * K * nst * tf["grad"], float(ph_mean[3])
         eval_flops = kern_flops + energy_flops
     ordered_equiv = K * K * nst * tf["grad"] + energy_flops
-    achieved = kern_flops / (kern_ms * 1e-3) / 1e12
-    traffic = None
+    # the roofline's FLOPs: the frozen per-term count (the current one is reported beside it)
+    per_frozen = frozen.get(per_term, tf[per_term])
+    terms_launch = kern_flops // tf[per_term]
+    achieved_current = kern_flops / (kern_ms * 1e-3) / 1e12
+    kern_flops_frozen = terms_launch * per_frozen
+    achieved = kern_flops_frozen / (kern_ms * 1e-3) / 1e12
+    traffic, traffic_src = None, None
     tpath = os.path.join(HERE, "profiles", "traffic.json")
     if os.path.exists(tpath):
         try:
-            traffic = json.load(open(tpath)).get(f"{kname}|{args.workload}")
+            tj = json.load(open(tpath))
+            traffic = tj.get(f"{kname}|{args.workload}")
+            traffic_src = tj.get("_source")
         except (OSError, ValueError):
             traffic = None
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
         cpu = cpu_port_rate(prob, args.cpu_seconds)
+    dropin = None
+    if world == 1 and not args.no_dropin:
+        dropin = dropin_figures(prob, e2e_value)
     served = None
     if world == 1 and args.serve_runs > 0:
         served = serving_figures(args.serve_runs, args.serve_maxfun, args.serve_procs)
@@ -351,24 +423,27 @@ def run_engine(args):
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded, oldquit.dat layout; no public dataset exists)",
-        "config": {"workload": args.workload, "desc": WORKLOADS[args.workload],
-                   "pair_elements_per_eval": prob.pairs, "terms_per_eval": (prob.pairs + K * K) * nst,
-                   "l2": "flushed between steps by a 256 MiB write, not timed",
-                   "pair_pass": ("fused energy + gradient, unordered pairs" if mode == 2 else
+        "config": bench_config(args, world),
+        "tuning": {"pair_pass": ("fused energy + gradient, unordered pairs" if mode == 2 else
                                  "energy pass + gradient over unordered pairs" if mode == 1 else
                                  "energy pass + gradient over ordered pairs"),
                    "tiles": {k: tiles.get(k, 1) for k in ("lc_e", "minb_e", "lc_g", "minb_g", "sym", "lc_s", "minw_s",
                                                           "npc")
-                             if k in tiles},
-                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+                             if k in tiles}},
+        "parity": parity,
         "pair_elements_per_s": value * prob.pairs,
         "energy": E,
         "phase_ms": dict(zip(PHASES, [round(float(v), 4) for v in ph_mean])),
         "roofline": {"bound": "fp64", "kernel": kname, "achieved": achieved, "peak": peak.value,
                      "unit": "TFLOP/s", "frac": achieved / peak.value, "traffic": traffic,
+                     "traffic_source": traffic_src,
+                     "flops_per_term_frozen": per_frozen,
+                     "achieved_at_current_count": achieved_current,
+                     "frac_at_current_count": achieved_current / peak.value,
+                     "kernel_ms": kern_ms,
                      "peak_source": "measured now by the FP64 FMA probe (necg_fp64_peak); "
                                     "MEASURED_PEAKS.json has no FP64 figure; nominal B200 FP64 = 37 TFLOP/s",
-                     "flops_per_launch": kern_flops, "flops_per_term": tf[per_term],
+                     "flops_per_launch": kern_flops_frozen, "flops_per_term": tf[per_term],
                      "special_per_term": tf[per_term + "_special"],
                      "energy_kernel": (None if mode == 2 else
                                        {"achieved": energy_flops / (float(ph_mean[1]) * 1e-3) / 1e12,
@@ -381,11 +456,43 @@ def run_engine(args):
         # status reset, 2 prep, pair pass(es), rows + finalize, partial sum(s), reduce
         "gpu_launches": (8 if mode == 2 else 9 if mode == 1 or (prob.K + tiles["lc_g"] - 1) // tiles["lc_g"] > 1
                          else 8) * args.steps,
-        "cpu_baseline": cpu,
+        "cpu_baseline": (dict(cpu, python_reference=python_reference_timing()) if cpu else None),
+        "dropin": dropin,
         "clocks": clk,
         "served": served,
     }
     print(json.dumps(out), flush=True)
+
+
+def dropin_figures(prob, e2e_value: float, calls: int = 20) -> dict:
+    """evals/s through the drop-in module API (shared module state + outprod,
+    the call python/necg.py:159-171 hands to the optimiser), host wall clock
+    around each call, with and without H and S copied back into shared."""
+    import tempfile
+
+    from nbo_correlatedgaussians_b200 import shared as sh
+    from nbo_correlatedgaussians_b200.outprod import outprod
+    from nbo_correlatedgaussians_b200.problem import write_oldquit
+    from nbo_correlatedgaussians_b200.read_input import read_input
+    with tempfile.TemporaryDirectory() as td:
+        fn = os.path.join(td, "oldquit.dat")
+        write_oldquit(prob, fn)
+        read_input(fn)
+    x = np.concatenate([sh.iv, sh.C])
+    out = {"path": "nbo_correlatedgaussians_b200.outprod.outprod (pageable numpy x in, f and g out)",
+           "calls": calls}
+    for sync in (False, True):
+        sh.sync_matrices = sync
+        for _ in range(3):
+            outprod(x)
+        t0 = time.perf_counter()
+        for _ in range(calls):
+            outprod(x)
+        rate = calls / (time.perf_counter() - t0)
+        out["sync_matrices" if sync else "no_sync_matrices"] = {"evals_per_s": rate,
+                                                              "vs_host_entry_e2e": rate / e2e_value}
+    sh.sync_matrices = True
+    return out
 
 
 def serving_figures(nruns: int, maxfun: int, procs: int = -1) -> dict:

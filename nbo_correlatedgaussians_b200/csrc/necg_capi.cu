@@ -131,7 +131,7 @@ void free_all(necg_handle *h) {
                     h->d_S, h->d_rows, h->d_scal, h->d_x, h->d_g, h->d_f, h->d_status,
                     h->d_tiles, h->d_pinv, h->d_kcnt, h->d_ksrc, h->d_kcoef, h->d_stiles,
                     h->d_stile_start, h->d_psym, h->d_sgroups, h->d_qcount, h->d_bgroups,
-                    h->d_Hp, h->d_Sp};
+                    h->d_Hp, h->d_Sp, h->d_xsym};
     for (void *p : ptrs) pool_free(h, p);
 }
 
@@ -208,7 +208,43 @@ int ensure_sym_tiles(necg_handle *h, int K, cudaStream_t st, int mult) {
     std::vector<int2> groups;  // gw consecutive ket chunks of one row block, largest blocks first
     for (int kb = nkb - 1; kb >= 0; --kb) {
         const int ntk = start[kb + 1] - start[kb];
-        for (int lc0 = 0; lc0 < ntk; lc0 += gw) groups.push_back(make_int2(kb, lc0));
+        for (int lc0 = 0; lc0 < ntk; lc0 += gw) groups.push_back(necg::sgroup_pack(kb, lc0, 0, 1));
+    }
+    // The groups are equal work, one block per SM takes them from the queue, so
+    // the last round runs G mod SMs groups while the other SMs idle: split each
+    // of those groups into `parts` units over the symmetry terms (as many as
+    // keep the round within one unit per SM, at most 4), so the last round is a
+    // part of a group long.
+    {
+        int sms = 148;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device);
+        const int G = (int)groups.size();
+        const int T = G % sms;
+        int parts = T > 0 ? sms / T : 1;
+        if (parts > 4) parts = 4;
+        if (parts > h->nst) parts = h->nst;
+        h->sg_ntail = 0;
+        h->sg_parts = 1;
+        h->sg_tail0 = G;
+        if (parts >= 2) {
+            std::vector<int2> tail(groups.end() - T, groups.end());
+            groups.resize(G - T);
+            for (const int2 &g : tail)
+                for (int q = 0; q < parts; ++q)
+                    groups.push_back(necg::sgroup_pack(g.x, necg::sgroup_lc0(g), q, parts));
+            h->sg_tail0 = G - T;
+            h->sg_ntail = T;
+            h->sg_parts = parts;
+            const size_t xneed = (size_t)T * gw * (parts - 1) * necg::fsym_tail_slot(PS, LC);
+            if (xneed > h->xsym_cap) {
+                pool_free(h, h->d_xsym, st);
+                h->d_xsym = nullptr;
+                h->xsym_cap = 0;
+                CK(pool_alloc(h, &h->d_xsym, xneed * sizeof(double), st));
+                h->ws_bytes += (long long)(xneed * sizeof(double));
+                h->xsym_cap = xneed;
+            }
+        }
     }
     if ((int)groups.size() > h->sgroups_cap) {
         pool_free(h, h->d_sgroups, st);
@@ -364,6 +400,10 @@ LaunchArgs base_args(necg_handle *h, int K) {
     a.sgroups = h->d_sgroups;
     a.nsgroups = h->nsgroups;
     a.qcount = h->d_qcount;
+    a.xsym = h->d_xsym;
+    a.sg_tail0 = h->sg_tail0;
+    a.sg_ntail = h->sg_ntail;
+    a.sg_parts = h->sg_parts;
     return a;
 }
 
@@ -574,10 +614,15 @@ int necg_outprod(necg_handle *h, int K, const double *x_dev, double *f_dev, doub
         a.npc = necg::fused_splits(h);
         a.Hp = h->d_Hp;
         a.Sp = h->d_Sp;
+        a.xsym = h->d_xsym;
+        a.sg_tail0 = h->sg_tail0;
+        a.sg_ntail = h->sg_ntail;
+        a.sg_parts = h->sg_parts;
         mark(h, 0, st);
         if (necg::launch_prep(a, st)) return NECG_ERR_UNSUPPORTED;
         mark(h, 1, st);
         if (necg::launch_fsym(a, st)) return NECG_ERR_ARG;
+        if (necg::launch_fsym_tail(a, st)) return NECG_ERR_ARG;
         if (necg::launch_hs_reduce(a, st)) return NECG_ERR_ARG;
         mark(h, 2, st);
         necg::launch_rows_finalize(a, f_dev, g_dev + siv, 0, 0.0, 0.0, st);

@@ -52,6 +52,17 @@ __device__ __forceinline__ void flag_status(int *status, int flags, int pair) {
     atomicMin(status + 1, pair);
 }
 
+// Where a part of a split tile of the lockstep pass writes instead of the
+// main buffers (slot < 0: the main buffers): slot `slot` of x, fsym_tail_slot
+// doubles holding its 2 PS 32 bra partials, then its LC x 2 PS ket partials,
+// then its LC x 64 H and S sums (H for the 32 bras, then S).  The address is
+// formed where it is used, so that it does not hold registers through the term
+// loop.
+struct TileOut {
+    double *x = nullptr;
+    int slot = -1;
+};
+
 // Shared memory of one warp's fused tile: bra accumulators for H and S
 // (2 * PS * 32 doubles), two ket tables of 16 rows (2 * 16 * 33) and one
 // reduction row (32).  Sized by the caller for its largest n.
@@ -88,7 +99,8 @@ struct FusedSmem {
 // (cp.async) runs while the current term is evaluated.
 // [p0, p1): the symmetry terms this tile takes (p1 < 0: all nst).  A pass whose
 // tiles split the terms writes each split's partials to its own slot (t is then
-// the slot index) and each split's H, S sums to its own K x K buffer.
+// the slot index) and each split's H, S sums to its own K x K buffer, or (xo)
+// to the compact buffers of one part of a split tile.
 // SYNC (with BSYNC): 0 -- every warp takes the block barrier at the end of
 // each term; 1, 2 -- warps 4-7 of the block take it inside the term instead
 // (at term_fused's mid(1): after B, Bi, T and ov; mid(2): after tau and sig),
@@ -101,7 +113,8 @@ __device__ __forceinline__ void fsym_tile(int t, int2 tl, int LC, int K, int nst
                                           double *__restrict__ H, double *__restrict__ S,
                                           double *__restrict__ part_b, double *__restrict__ part_k,
                                           int *status, FusedSmem sm, bool idle = false,
-                                          const double *sbra = nullptr, int p0 = 0, int p1 = -1) {
+                                          const double *sbra = nullptr, int p0 = 0, int p1 = -1,
+                                          TileOut xo = TileOut{}) {
     using KL = KetLayout<N>;
     constexpr int PS = Part<N>::size;
     static_assert(PS <= 32, "the symmetric pass needs tri(n) + 1 + 3n <= 32");
@@ -226,19 +239,29 @@ __device__ __forceinline__ void fsym_tile(int t, int2 tl, int LC, int K, int nst
                 bad = min(bad, k * K + l);
                 flags |= 2;
             }
-            H[(size_t)k * K + l] = hsum;
-            H[(size_t)l * K + k] = hsum;
-            S[(size_t)k * K + l] = ssum;
-            S[(size_t)l * K + k] = ssum;
+            if (xo.slot >= 0) {
+                double *hs = xo.x + (size_t)xo.slot * fsym_tail_slot(PS, LC) + 2 * PS * 32 + (size_t)LC * 2 * PS;
+                hs[(l - l0) * 64 + lane] = hsum;
+                hs[(l - l0) * 64 + 32 + lane] = ssum;
+            } else {
+                H[(size_t)k * K + l] = hsum;
+                H[(size_t)l * K + k] = hsum;
+                S[(size_t)k * K + l] = ssum;
+                S[(size_t)l * K + k] = ssum;
+            }
         }
         if (lane < PS) {
-            part_k[(((size_t)t * LC + (l - l0)) * 2 + 0) * PS + lane] = aH;
-            part_k[(((size_t)t * LC + (l - l0)) * 2 + 1) * PS + lane] = aS;
+            double *pk = xo.slot >= 0 ? xo.x + (size_t)xo.slot * fsym_tail_slot(PS, LC) + 2 * PS * 32 +
+                                            (size_t)(l - l0) * 2 * PS
+                                      : part_k + ((size_t)t * LC + (l - l0)) * 2 * PS;
+            pk[lane] = aH;
+            pk[PS + lane] = aS;
         }
     }
     if (kval) {
+        double *pb = xo.slot >= 0 ? xo.x + (size_t)xo.slot * fsym_tail_slot(PS, LC) : part_b + (size_t)t * 2 * PS * 32;
 #pragma unroll
-        for (int f = 0; f < 2 * PS; ++f) part_b[((size_t)t * 2 * PS + f) * 32 + lane] = sm.sacc[f * 32 + lane];
+        for (int f = 0; f < 2 * PS; ++f) pb[f * 32 + lane] = sm.sacc[f * 32 + lane];
     }
     if (!ok) flags |= 1;
     flag_status(status, flags, bad);

@@ -40,6 +40,11 @@ struct necg_handle {
     size_t psym_cap = 0;  // doubles
     int2 *d_sgroups = nullptr;  // groups of 8 fused tiles of one row block (kb, first lc)
     int sgroups_cap = 0, nsgroups = 0, sgroups_w = 0;
+    // the queue's tail: its last sg_ntail groups split into sg_parts units from
+    // queue index sg_tail0; parts after the first write to d_xsym
+    int sg_tail0 = 0, sg_ntail = 0, sg_parts = 1;
+    double *d_xsym = nullptr;
+    size_t xsym_cap = 0;  // doubles
     int *d_qcount = nullptr;    // queue head of the block-synchronised fused pass
     int2 *d_bgroups = nullptr;  // the same groups with 8 chunks each (the batched step's blocks)
     int bgroups_cap = 0, nbgroups = 0;

@@ -342,7 +342,8 @@ __global__ void __launch_bounds__(32 * WARPS, 1) fsym_block_kernel(const int2 *_
                                                                 const double *__restrict__ C, KetMap kmap,
                                                                 double *__restrict__ H, double *__restrict__ S,
                                                                 double *__restrict__ part_b,
-                                                                double *__restrict__ part_k, int *status) {
+                                                                double *__restrict__ part_k, int *status,
+                                                                double *__restrict__ xsym, int tail0) {
     extern __shared__ __align__(16) double smem[];
     __shared__ int gsh;
     constexpr int PS = Part<N>::size;
@@ -360,9 +361,18 @@ __global__ void __launch_bounds__(32 * WARPS, 1) fsym_block_kernel(const int2 *_
         __syncthreads();  // every thread has read gsh before it changes
         if (g >= ngroups) break;
         const int2 gr = groups[g];
-        const int kb = gr.x, lc = gr.y + w;
+        const int kb = gr.x, lc = sgroup_lc0(gr) + w;
         const int last = min(kb * 32 + 31, K - 1);
         const bool idle = lc * LC > last;  // past this block's triangle: barriers only
+        // a split group of the queue's tail: this unit takes symmetry terms
+        // [p0, p1); parts after the first write to their own slots in xsym
+        const int part = sgroup_part(gr), parts = sgroup_parts(gr);
+        const int PC = (nst + parts - 1) / parts, p0 = min(part * PC, nst), p1 = min(p0 + PC, nst);
+        TileOut xo;
+        if (part > 0) {
+            xo.x = xsym;
+            xo.slot = (((g - tail0) / parts) * WARPS + w) * (parts - 1) + (part - 1);
+        }
         if constexpr (SBRA) {  // the group's 32 bras, once for all warps
             for (int i = threadIdx.x; i < BS * 32; i += 32 * WARPS) {
                 const int f = i >> 5, kk = min(kb * 32 + (i & 31), K - 1);
@@ -371,8 +381,54 @@ __global__ void __launch_bounds__(32 * WARPS, 1) fsym_block_kernel(const int2 *_
             __syncthreads();
         }
         fsym_tile<N, VKET, true, SBRA, SKET, SYNC>(tstart[kb] + lc, make_int2(kb, lc), LC, K, nst, cs, bra, ket, C,
-                                                   kmap, H, S, part_b, part_k, status, sm, idle, sbra);
+                                                   kmap, H, S, part_b, part_k, status, sm, idle, sbra, p0, p1, xo);
         if constexpr (SBRA) __syncthreads();  // sbra is rewritten for the next group
+    }
+}
+
+// The split tail of the lockstep pass: add parts 1 .. parts - 1 of each tile
+// (their compact slots in xsym, in part order) into the tile's main partials
+// and H, S entries, which part 0 wrote.  Block = one tile (tail group j, warp
+// w); entries that no part wrote (lanes past K, kets past K or above the
+// diagonal, tiles past the block's triangle) are left alone.
+template <int N>
+__global__ void __launch_bounds__(256) fsym_tail_fix_kernel(const int2 *__restrict__ groups, int tail0, int W,
+                                                            int LC, int K, const int *__restrict__ tstart,
+                                                            const double *__restrict__ xsym,
+                                                            double *__restrict__ part_b, double *__restrict__ part_k,
+                                                            double *__restrict__ H, double *__restrict__ S) {
+    constexpr int PS = Part<N>::size;
+    const int j = blockIdx.x / W, w = blockIdx.x - j * W;
+    const int2 gr = groups[tail0 + j * sgroup_parts(groups[tail0])];
+    const int parts = sgroup_parts(gr);
+    const int kb = gr.x, lc = sgroup_lc0(gr) + w;
+    const int last = min(kb * 32 + 31, K - 1);
+    if (lc * LC > last) return;
+    const int t = tstart[kb] + lc;
+    const size_t XS = fsym_tail_slot(PS, LC);
+    const double *x0 = xsym + (size_t)(j * W + w) * (parts - 1) * XS;
+    double *pb = part_b + (size_t)t * 2 * PS * 32;
+    for (int i = threadIdx.x; i < 2 * PS * 32; i += blockDim.x) {
+        if (kb * 32 + (i & 31) >= K) continue;
+        double v = pb[i];
+        for (int q = 0; q < parts - 1; ++q) v += x0[q * XS + i];
+        pb[i] = v;
+    }
+    double *pk = part_k + (size_t)t * LC * 2 * PS;
+    for (int i = threadIdx.x; i < LC * 2 * PS; i += blockDim.x) {
+        if (lc * LC + i / (2 * PS) >= K) continue;
+        double v = pk[i];
+        for (int q = 0; q < parts - 1; ++q) v += x0[q * XS + 2 * PS * 32 + i];
+        pk[i] = v;
+    }
+    for (int i = threadIdx.x; i < LC * 64; i += blockDim.x) {
+        const int l = lc * LC + i / 64, r = i & 63, k = kb * 32 + (r & 31);
+        if (k >= K || l >= K || l > k) continue;
+        double *M = r < 32 ? H : S;
+        double v = M[(size_t)k * K + l];
+        for (int q = 0; q < parts - 1; ++q) v += x0[q * XS + 2 * PS * 32 + (size_t)LC * 2 * PS + i];
+        M[(size_t)k * K + l] = v;
+        M[(size_t)l * K + k] = v;
     }
 }
 
@@ -788,7 +844,8 @@ template <int N> struct Launch {
                 if (grid < 1) return;
                 kern<<<grid, 32 * WARPS, smem, st>>>(a.sgroups, a.nsgroups, a.qcount, a.stile_start, a.LC_s, a.K,
                                                      a.nst, cs, a.bra, a.ket, a.C, a.kmap, a.H, a.S, a.psym,
-                                                     a.psym + (size_t)a.nstiles * 2 * Part<N>::size * 32, a.status);
+                                                     a.psym + (size_t)a.nstiles * 2 * Part<N>::size * 32, a.status,
+                                                     a.xsym, a.sg_tail0);
             }
         }
     }
@@ -814,6 +871,14 @@ template <int N> struct Launch {
         case 118: fsym_v<8, true, true>(a, st); break;
         case 122: fsym_v<12, true, true>(a, st); break;
         default: fsym_v<8, false>(a, st); break;
+        }
+    }
+    static void fsym_tail(const LaunchArgs &a, cudaStream_t st) {
+        if constexpr (Part<N>::size <= 32) {
+            const int W = fused_block_warps(a.minb_s);
+            fsym_tail_fix_kernel<N><<<a.sg_ntail * W, 256, 0, st>>>(
+                a.sgroups, a.sg_tail0, W, a.LC_s, a.K, a.stile_start, a.xsym, a.psym,
+                a.psym + (size_t)a.nstiles * 2 * Part<N>::size * 32, a.H, a.S);
         }
     }
     static void fsym_reduce(const LaunchArgs &a, cudaStream_t st) {
@@ -920,6 +985,13 @@ int launch_fsym(const LaunchArgs &a, cudaStream_t st) {
     // every buffer the pass writes must be set (no launch on a null pointer)
     if (!a.H || !a.S || !a.psym || !a.stiles || !a.bra || !a.ket || !a.C || !a.status) return -1;
     NECG_DISPATCH(a.n, fsym_tiles(a, st));
+    return 0;
+}
+int launch_fsym_tail(const LaunchArgs &a, cudaStream_t st) {
+    // only the lockstep pass over the whole tile list splits its tail
+    if (a.minb_s < 200 || a.st_end > 0 || a.sg_ntail <= 0 || a.sg_parts < 2) return 0;
+    if (a.n > 5 || !a.sgroups || !a.xsym || !a.psym || !a.H || !a.S || !a.stile_start) return -1;
+    NECG_DISPATCH(a.n, fsym_tail(a, st));
     return 0;
 }
 int launch_fsym_reduce(const LaunchArgs &a, cudaStream_t st) {

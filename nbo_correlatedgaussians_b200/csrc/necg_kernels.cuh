@@ -39,7 +39,23 @@ struct LaunchArgs {
     // variants; npc <= 1: no split): split pc writes its H, S sums to Hp, Sp + pc K^2
     int npc;
     double *Hp, *Sp;
+    // lockstep pass: the last sg_ntail groups of the queue are split into
+    // sg_parts units over the symmetry terms, from queue index sg_tail0; parts
+    // 1 .. sg_parts - 1 write to xsym (fsym_tail_slot doubles per tile and part)
+    double *xsym;
+    int sg_tail0, sg_ntail, sg_parts;
 };
+
+// A tile group of the lockstep pass: row block kb, first ket chunk lc0 and, for
+// a split group of the queue's tail, its part and the number of parts (one part
+// per range of symmetry terms).
+__host__ __device__ inline int2 sgroup_pack(int kb, int lc0, int part, int parts) {
+    return make_int2(kb, lc0 | (part << 20) | (parts << 24));
+}
+__host__ __device__ inline int sgroup_lc0(int2 g) { return g.y & 0xFFFFF; }
+__host__ __device__ inline int sgroup_part(int2 g) { return (g.y >> 20) & 0xF; }
+__host__ __device__ inline int sgroup_parts(int2 g) { return ((g.y >> 24) & 0xF) > 1 ? ((g.y >> 24) & 0xF) : 1; }
+
 
 int launch_prep(const LaunchArgs &a, cudaStream_t st);
 int launch_energy(const LaunchArgs &a, cudaStream_t st);
@@ -56,6 +72,9 @@ bool fused_variant_ok(int n, int variant);
 int launch_fsym_reduce(const LaunchArgs &a, cudaStream_t st);
 // H, S = sum over the splits of Hp, Sp (fused pass with npc > 1), before rows/finalize
 int launch_hs_reduce(const LaunchArgs &a, cudaStream_t st);
+// add the split parts of the lockstep pass's tail tiles into the main buffers
+// (after launch_fsym, before H and S are read)
+int launch_fsym_tail(const LaunchArgs &a, cudaStream_t st);
 int launch_grad_tiles(const LaunchArgs &a, cudaStream_t st);
 int launch_grad_reduce(const LaunchArgs &a, cudaStream_t st);
 int launch_matel(const LaunchArgs &a, const int *terms, int nterms, double *out, cudaStream_t st);
