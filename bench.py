@@ -454,14 +454,36 @@ def run_engine(args):
                 "d2h_bytes_per_step": int(prob.x.nbytes) + 8,
                 "path": "necg_outprod_host (pinned host x -> f, g)"},
         # status reset, 2 prep, pair pass(es), rows + finalize, partial sum(s), reduce
-        "gpu_launches": (8 if mode == 2 else 9 if mode == 1 or (prob.K + tiles["lc_g"] - 1) // tiles["lc_g"] > 1
-                         else 8) * args.steps,
+        "gpu_launches": launches_per_eval(prob, tiles, mode) * args.steps,
         "cpu_baseline": (dict(cpu, python_reference=python_reference_timing()) if cpu else None),
         "dropin": dropin,
         "clocks": clk,
         "served": served,
     }
     print(json.dumps(out), flush=True)
+
+
+def launches_per_eval(prob, tiles: dict, mode: int) -> int:
+    """Library kernels one evaluation launches: status reset, bra and ket
+    records, the pair pass(es), H C / S C rows, finalize, partial sum(s) and the
+    reduce to the parameter layout; in the fused pass also the fix-up of the
+    lockstep queue's split tail, or the sum of split H, S of one-warp tiles."""
+    import torch
+    K, nst = prob.K, prob.nst
+    if mode != 2:
+        return 9 if mode == 1 or (K + tiles["lc_g"] - 1) // tiles["lc_g"] > 1 else 8
+    n = 8
+    minw, lc = int(tiles.get("minw_s", 8)), int(tiles.get("lc_s", 2))
+    if minw >= 200:  # lockstep groups: the tail is split when the last round is partial
+        gw = 12 if minw in (222, 232) else 8
+        groups = sum(-(-(min(kb * 32 + 31, K - 1) // lc + 1) // gw) for kb in range((K + 31) // 32))
+        sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+        tail = groups % sms
+        if tail and min(4, nst, sms // tail) >= 2:
+            n += 1
+    elif int(tiles.get("npc", 1)) > 1:
+        n += 1
+    return n
 
 
 def dropin_figures(prob, e2e_value: float, calls: int = 20) -> dict:
