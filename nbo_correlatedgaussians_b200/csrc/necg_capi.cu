@@ -131,7 +131,7 @@ void free_all(necg_handle *h) {
                     h->d_S, h->d_rows, h->d_scal, h->d_x, h->d_g, h->d_f, h->d_status,
                     h->d_tiles, h->d_pinv, h->d_kcnt, h->d_ksrc, h->d_kcoef, h->d_stiles,
                     h->d_stile_start, h->d_psym, h->d_sgroups, h->d_qcount, h->d_bgroups,
-                    h->d_Hp, h->d_Sp, h->d_xsym};
+                    h->d_Hp, h->d_Sp, h->d_xsym, h->d_urange};
     for (void *p : ptrs) pool_free(h, p);
 }
 
@@ -223,6 +223,9 @@ int ensure_sym_tiles(necg_handle *h, int K, cudaStream_t st, int mult) {
         int parts = T > 0 ? sms / T : 1;
         if (parts > 4) parts = 4;
         if (parts > h->nst) parts = h->nst;
+        // the lockstep pass writes bra partials per queue unit into the slots
+        // sized for the tiles: G - T + T parts units must not exceed them
+        if (T > 0 && parts > 1 + ((int)t.size() - G) / T) parts = 1 + ((int)t.size() - G) / T;
         h->sg_ntail = 0;
         h->sg_parts = 1;
         h->sg_tail0 = G;
@@ -253,6 +256,21 @@ int ensure_sym_tiles(necg_handle *h, int K, cudaStream_t st, int mult) {
         h->sgroups_cap = (int)groups.size();
     }
     if (!h->d_qcount) CK(pool_alloc(h, &h->d_qcount, sizeof(int), st));
+    // each row block's queue units are contiguous (blocks in decreasing order,
+    // a split group's parts next to each other)
+    std::vector<int2> urange(nkb, make_int2(0, 0));
+    for (int u = 0; u < (int)groups.size(); ++u) {
+        int2 &r = urange[groups[u].x];
+        if (r.y == 0) r.x = u;
+        r.y = u + 1;
+    }
+    if (nkb > h->urange_cap) {
+        pool_free(h, h->d_urange, st);
+        h->d_urange = nullptr;
+        CK(pool_alloc(h, &h->d_urange, nkb * sizeof(int2), st));
+        h->urange_cap = nkb;
+    }
+    CK(cudaMemcpyAsync(h->d_urange, urange.data(), nkb * sizeof(int2), cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(h->d_sgroups, groups.data(), groups.size() * sizeof(int2), cudaMemcpyHostToDevice, st));
     h->nsgroups = (int)groups.size();
     h->sgroups_w = gw;
@@ -404,6 +422,7 @@ LaunchArgs base_args(necg_handle *h, int K) {
     a.sg_tail0 = h->sg_tail0;
     a.sg_ntail = h->sg_ntail;
     a.sg_parts = h->sg_parts;
+    a.urange = h->d_urange;
     return a;
 }
 
@@ -618,6 +637,7 @@ int necg_outprod(necg_handle *h, int K, const double *x_dev, double *f_dev, doub
         a.sg_tail0 = h->sg_tail0;
         a.sg_ntail = h->sg_ntail;
         a.sg_parts = h->sg_parts;
+        a.urange = h->d_urange;
         mark(h, 0, st);
         if (necg::launch_prep(a, st)) return NECG_ERR_UNSUPPORTED;
         mark(h, 1, st);

@@ -54,10 +54,9 @@ __device__ __forceinline__ void flag_status(int *status, int flags, int pair) {
 
 // Where a part of a split tile of the lockstep pass writes instead of the
 // main buffers (slot < 0: the main buffers): slot `slot` of x, fsym_tail_slot
-// doubles holding its 2 PS 32 bra partials, then its LC x 2 PS ket partials,
-// then its LC x 64 H and S sums (H for the 32 bras, then S).  The address is
-// formed where it is used, so that it does not hold registers through the term
-// loop.
+// doubles holding its LC x 2 PS ket partials, then its LC x 64 H and S sums (H
+// for the 32 bras, then S).  The address is formed where it is used, so that
+// it does not hold registers through the term loop.
 struct TileOut {
     double *x = nullptr;
     int slot = -1;
@@ -101,12 +100,14 @@ struct FusedSmem {
 // tiles split the terms writes each split's partials to its own slot (t is then
 // the slot index) and each split's H, S sums to its own K x K buffer, or (xo)
 // to the compact buffers of one part of a split tile.
+// WB: write the bra partials to part_b (false: the caller reduces the warps'
+// accumulators, left in sm.sacc, itself).
 // SYNC (with BSYNC): 0 -- every warp takes the block barrier at the end of
 // each term; 1, 2 -- warps 4-7 of the block take it inside the term instead
 // (at term_fused's mid(1): after B, Bi, T and ov; mid(2): after tau and sig),
 // so the two warps of each scheduler run different stretches of the body; 3 --
 // no barrier per term (the warps only meet at the tile group's barriers).
-template <int N, bool VKET, bool BSYNC = false, bool SBRA = false, bool SKET = false, int SYNC = 0>
+template <int N, bool VKET, bool BSYNC = false, bool SBRA = false, bool SKET = false, int SYNC = 0, bool WB = true>
 __device__ __forceinline__ void fsym_tile(int t, int2 tl, int LC, int K, int nst, const Consts<N> &cs,
                                           const double *__restrict__ bra, const double *__restrict__ ket,
                                           const double *__restrict__ C, const KetMap &kmap,
@@ -240,7 +241,7 @@ __device__ __forceinline__ void fsym_tile(int t, int2 tl, int LC, int K, int nst
                 flags |= 2;
             }
             if (xo.slot >= 0) {
-                double *hs = xo.x + (size_t)xo.slot * fsym_tail_slot(PS, LC) + 2 * PS * 32 + (size_t)LC * 2 * PS;
+                double *hs = xo.x + (size_t)xo.slot * fsym_tail_slot(PS, LC) + (size_t)LC * 2 * PS;
                 hs[(l - l0) * 64 + lane] = hsum;
                 hs[(l - l0) * 64 + 32 + lane] = ssum;
             } else {
@@ -251,15 +252,14 @@ __device__ __forceinline__ void fsym_tile(int t, int2 tl, int LC, int K, int nst
             }
         }
         if (lane < PS) {
-            double *pk = xo.slot >= 0 ? xo.x + (size_t)xo.slot * fsym_tail_slot(PS, LC) + 2 * PS * 32 +
-                                            (size_t)(l - l0) * 2 * PS
+            double *pk = xo.slot >= 0 ? xo.x + (size_t)xo.slot * fsym_tail_slot(PS, LC) + (size_t)(l - l0) * 2 * PS
                                       : part_k + ((size_t)t * LC + (l - l0)) * 2 * PS;
             pk[lane] = aH;
             pk[PS + lane] = aS;
         }
     }
-    if (kval) {
-        double *pb = xo.slot >= 0 ? xo.x + (size_t)xo.slot * fsym_tail_slot(PS, LC) : part_b + (size_t)t * 2 * PS * 32;
+    if (WB && kval) {
+        double *pb = part_b + (size_t)t * 2 * PS * 32;
 #pragma unroll
         for (int f = 0; f < 2 * PS; ++f) pb[f * 32 + lane] = sm.sacc[f * 32 + lane];
     }

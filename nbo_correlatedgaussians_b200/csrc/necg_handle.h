@@ -45,6 +45,8 @@ struct necg_handle {
     int sg_tail0 = 0, sg_ntail = 0, sg_parts = 1;
     double *d_xsym = nullptr;
     size_t xsym_cap = 0;  // doubles
+    int2 *d_urange = nullptr;  // queue units of each row block (bra partial slots)
+    int urange_cap = 0;
     int *d_qcount = nullptr;    // queue head of the block-synchronised fused pass
     int2 *d_bgroups = nullptr;  // the same groups with 8 chunks each (the batched step's blocks)
     int bgroups_cap = 0, nbgroups = 0;

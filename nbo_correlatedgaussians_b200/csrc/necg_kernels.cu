@@ -380,23 +380,36 @@ __global__ void __launch_bounds__(32 * WARPS, 1) fsym_block_kernel(const int2 *_
             }
             __syncthreads();
         }
-        fsym_tile<N, VKET, true, SBRA, SKET, SYNC>(tstart[kb] + lc, make_int2(kb, lc), LC, K, nst, cs, bra, ket, C,
-                                                   kmap, H, S, part_b, part_k, status, sm, idle, sbra, p0, p1, xo);
+        fsym_tile<N, VKET, true, SBRA, SKET, SYNC, false>(tstart[kb] + lc, make_int2(kb, lc), LC, K, nst, cs, bra,
+                                                          ket, C, kmap, H, S, part_b, part_k, status, sm, idle,
+                                                          sbra, p0, p1, xo);
+        // the group's bra partials: its warps share the 32 bras, so their
+        // accumulators are summed (in warp order) and written once, to the
+        // slot of queue unit g
+        __syncthreads();
+        for (int i = threadIdx.x; i < 2 * PS * 32; i += 32 * WARPS) {
+            if (kb * 32 + (i & 31) >= K) continue;
+            double v = smem[i];
+#pragma unroll
+            for (int q = 1; q < WARPS; ++q) v += smem[q * PER_WARP + i];
+            part_b[(size_t)g * 2 * PS * 32 + i] = v;
+        }
         if constexpr (SBRA) __syncthreads();  // sbra is rewritten for the next group
     }
 }
 
 // The split tail of the lockstep pass: add parts 1 .. parts - 1 of each tile
-// (their compact slots in xsym, in part order) into the tile's main partials
-// and H, S entries, which part 0 wrote.  Block = one tile (tail group j, warp
-// w); entries that no part wrote (lanes past K, kets past K or above the
-// diagonal, tiles past the block's triangle) are left alone.
+// (their compact slots in xsym, in part order) into the tile's ket partials
+// and H, S entries, which part 0 wrote (each part's bra partials have a queue
+// slot of their own).  Block = one tile (tail group j, warp w); entries that no
+// part wrote (kets past K or above the diagonal, tiles past the block's
+// triangle) are left alone.
 template <int N>
 __global__ void __launch_bounds__(256) fsym_tail_fix_kernel(const int2 *__restrict__ groups, int tail0, int W,
                                                             int LC, int K, const int *__restrict__ tstart,
                                                             const double *__restrict__ xsym,
-                                                            double *__restrict__ part_b, double *__restrict__ part_k,
-                                                            double *__restrict__ H, double *__restrict__ S) {
+                                                            double *__restrict__ part_k, double *__restrict__ H,
+                                                            double *__restrict__ S) {
     constexpr int PS = Part<N>::size;
     const int j = blockIdx.x / W, w = blockIdx.x - j * W;
     const int2 gr = groups[tail0 + j * sgroup_parts(groups[tail0])];
@@ -407,18 +420,11 @@ __global__ void __launch_bounds__(256) fsym_tail_fix_kernel(const int2 *__restri
     const int t = tstart[kb] + lc;
     const size_t XS = fsym_tail_slot(PS, LC);
     const double *x0 = xsym + (size_t)(j * W + w) * (parts - 1) * XS;
-    double *pb = part_b + (size_t)t * 2 * PS * 32;
-    for (int i = threadIdx.x; i < 2 * PS * 32; i += blockDim.x) {
-        if (kb * 32 + (i & 31) >= K) continue;
-        double v = pb[i];
-        for (int q = 0; q < parts - 1; ++q) v += x0[q * XS + i];
-        pb[i] = v;
-    }
     double *pk = part_k + (size_t)t * LC * 2 * PS;
     for (int i = threadIdx.x; i < LC * 2 * PS; i += blockDim.x) {
         if (lc * LC + i / (2 * PS) >= K) continue;
         double v = pk[i];
-        for (int q = 0; q < parts - 1; ++q) v += x0[q * XS + 2 * PS * 32 + i];
+        for (int q = 0; q < parts - 1; ++q) v += x0[q * XS + i];
         pk[i] = v;
     }
     for (int i = threadIdx.x; i < LC * 64; i += blockDim.x) {
@@ -426,7 +432,7 @@ __global__ void __launch_bounds__(256) fsym_tail_fix_kernel(const int2 *__restri
         if (k >= K || l >= K || l > k) continue;
         double *M = r < 32 ? H : S;
         double v = M[(size_t)k * K + l];
-        for (int q = 0; q < parts - 1; ++q) v += x0[q * XS + 2 * PS * 32 + (size_t)LC * 2 * PS + i];
+        for (int q = 0; q < parts - 1; ++q) v += x0[q * XS + (size_t)LC * 2 * PS + i];
         M[(size_t)k * K + l] = v;
         M[(size_t)l * K + k] = v;
     }
@@ -444,14 +450,17 @@ __global__ void __launch_bounds__(256) fsym_sum_kernel(const int *__restrict__ t
                                                        const double *__restrict__ part_b,
                                                        const double *__restrict__ part_k,
                                                        const double *__restrict__ scal,
-                                                       double *__restrict__ out, int t0, int t1, int npc) {
+                                                       double *__restrict__ out, int t0, int t1, int npc,
+                                                       const int2 *__restrict__ urange) {
     constexpr int PS = Part<N>::size;
     __shared__ double red[2][8][32];
     const int kb = blockIdx.x, f = blockIdx.y;
     const int lane = threadIdx.x & 31, seg = threadIdx.x >> 5;
     const int m = kb * 32 + lane;
-    // partial slots: tile t's splits are slots t npc .. t npc + npc - 1
-    const int ta = max(tstart[kb], t0) * npc, tb = min(tstart[kb + 1], t1) * npc;
+    // bra partial slots: tile t's splits are slots t npc .. t npc + npc - 1, or
+    // (urange, the lockstep pass) the queue units [urange[kb].x, urange[kb].y)
+    const int ta = urange ? urange[kb].x : max(tstart[kb], t0) * npc;
+    const int tb = urange ? urange[kb].y : min(tstart[kb + 1], t1) * npc;
     double sH = 0.0, sS = 0.0;
     for (int t = ta + seg; t < tb; t += 8) {
         sH += part_b[(((size_t)t * 2 + 0) * PS + f) * 32 + lane];
@@ -877,7 +886,7 @@ template <int N> struct Launch {
         if constexpr (Part<N>::size <= 32) {
             const int W = fused_block_warps(a.minb_s);
             fsym_tail_fix_kernel<N><<<a.sg_ntail * W, 256, 0, st>>>(
-                a.sgroups, a.sg_tail0, W, a.LC_s, a.K, a.stile_start, a.xsym, a.psym,
+                a.sgroups, a.sg_tail0, W, a.LC_s, a.K, a.stile_start, a.xsym,
                 a.psym + (size_t)a.nstiles * 2 * Part<N>::size * 32, a.H, a.S);
         }
     }
@@ -886,9 +895,12 @@ template <int N> struct Launch {
             constexpr int PS = Part<N>::size;
             const int t0 = a.st_end > 0 ? a.st_begin : 0, t1 = a.st_end > 0 ? a.st_end : a.nstiles;
             const int npc = a.npc > 1 && a.minb_s < 200 ? a.npc : 1;
+            // the lockstep pass over the whole tile list writes its bra partials
+            // per queue unit (the unit ranges of each row block in urange)
+            const bool lockstep = a.minb_s >= 200 && a.st_end == 0 && a.sgroups && a.urange;
             fsym_sum_kernel<N><<<dim3((a.K + 31) / 32, PS), 256, 0, st>>>(
                 a.stile_start, a.LC_s, a.K, a.psym, a.psym + (size_t)a.nstiles * npc * 2 * PS * 32, a.scal,
-                a.sums ? a.sums : a.part, t0, t1, npc);
+                a.sums ? a.sums : a.part, t0, t1, npc, lockstep ? a.urange : nullptr);
             if (!a.sums)
                 grad_reduce_kernel<N><<<(a.K + 127) / 128, 128, 0, st>>>(a.part, a.K, a.bra, a.C, a.scal, a.g,
                                                                           a.status);

@@ -44,6 +44,9 @@ struct LaunchArgs {
     // 1 .. sg_parts - 1 write to xsym (fsym_tail_slot doubles per tile and part)
     double *xsym;
     int sg_tail0, sg_ntail, sg_parts;
+    // lockstep pass: bra partials are written per queue unit; row block kb's
+    // units are [urange[kb].x, urange[kb].y)
+    const int2 *urange;
 };
 
 // A tile group of the lockstep pass: row block kb, first ket chunk lc0 and, for

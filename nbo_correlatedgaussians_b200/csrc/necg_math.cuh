@@ -113,10 +113,10 @@ template <int N> struct Consts {
 };
 
 // Doubles of one part's compact output for one tile of a split lockstep group
-// of the fused pass (ps = tri(n) + 1 + 3n fields, lc kets per tile): bra
-// partials, ket partials, H and S sums.
+// of the fused pass (ps = tri(n) + 1 + 3n fields, lc kets per tile): ket
+// partials, then H and S sums.
 __host__ __device__ inline size_t fsym_tail_slot(int ps, int lc) {
-    return (size_t)2 * ps * 32 + (size_t)lc * 2 * ps + (size_t)lc * 64;
+    return (size_t)lc * 2 * ps + (size_t)lc * 64;
 }
 
 // Coulomb pair enumeration order: for q = 1..N, p = 0..q-1  -> index q(q-1)/2 + p
