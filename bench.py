@@ -71,6 +71,7 @@ def parse():
                          "latency / throughput figures; 0 skips them")
     ap.add_argument("--serve-maxfun", type=int, default=50, help="evaluations per run of that stream")
     ap.add_argument("--no-dropin", action="store_true", help="skip the drop-in module figure")
+    ap.add_argument("--no-batched", action="store_true", help="skip the 64-instance batched figure")
     ap.add_argument("--serve-procs", type=int, default=-1,
                     help="client processes for the served figures (0: clients as threads of the bench process; "
                          "default: min(12, host cores - 2))")
@@ -415,6 +416,9 @@ def run_engine(args):
     dropin = None
     if world == 1 and not args.no_dropin:
         dropin = dropin_figures(prob, e2e_value)
+    batched = None
+    if world == 1 and not args.no_batched:
+        batched = batched_figures()
     served = None
     if world == 1 and args.serve_runs > 0:
         served = serving_figures(args.serve_runs, args.serve_maxfun, args.serve_procs)
@@ -457,6 +461,7 @@ def run_engine(args):
         "gpu_launches": launches_per_eval(prob, tiles, mode) * args.steps,
         "cpu_baseline": (dict(cpu, python_reference=python_reference_timing()) if cpu else None),
         "dropin": dropin,
+        "batched": batched,
         "clocks": clk,
         "served": served,
     }
@@ -484,6 +489,50 @@ def launches_per_eval(prob, tiles: dict, mode: int) -> int:
     elif int(tiles.get("npc", 1)) > 1:
         n += 1
     return n
+
+
+def batched_figures(steps: int = 10) -> dict:
+    """The 64-instance mixed batch (16 He with K log-uniform 32-512, 24 H2 and 24
+    LiH with K 64-1024; seeds 3000 + i): one batched step (a persistent launch
+    over every instance's tiles, replayed as a CUDA graph) against the same
+    instances evaluated one after another through the per-call path, each with
+    its autotuned setting; x resident on the device, CUDA events on the stream."""
+    import torch
+
+    from nbo_correlatedgaussians_b200 import _lib, synth
+    from nbo_correlatedgaussians_b200.batch import BatchEngine
+    probs = synth.workload("mixed64")
+    be = BatchEngine(probs, tune=True)
+    L = _lib.lib()
+    stream = torch.cuda.current_stream()
+    be.plan()
+
+    def timed(fn) -> float:
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    def per_call():
+        for i, eng in enumerate(be.engines):
+            _lib.check(L.necg_outprod(eng.h, probs[i].K, be.x[i].data_ptr(), be.f[i].data_ptr(), be.g[i].data_ptr(),
+                                      None, None, stream.cuda_stream), "necg_outprod")
+
+    batch_ms = timed(lambda: be.step(graph=True))
+    be.check()
+    call_ms = timed(per_call)
+    n = len(probs)
+    be.close()
+    return {"workload": "mixed64: 16 He (K 32-512), 24 H2 and 24 LiH (K 64-1024), seeds 3000+i", "instances": n,
+            "batched_ms_per_step": batch_ms, "batched_evals_per_s": n / (batch_ms * 1e-3),
+            "per_call_ms_per_round": call_ms, "per_call_evals_per_s": n / (call_ms * 1e-3),
+            "batched_vs_per_call": call_ms / batch_ms}
 
 
 def dropin_figures(prob, e2e_value: float, calls: int = 20) -> dict:
