@@ -171,7 +171,7 @@ __global__ void __launch_bounds__(32) batch_energy_kernel(PlanPtrs p) {
 __global__ void __launch_bounds__(32, 8) batch_fused_warp_kernel(PlanPtrs p) {
     __shared__ double sacc[2 * Part<kMaxN>::size * 32];
     __shared__ double krow[2 * 16 * 33];
-    __shared__ double kred[32];
+    __shared__ double kred[64];
     const int lane = threadIdx.x & 31;
     const int nf = p.hdr->nf;
     for (;;) {
@@ -202,7 +202,7 @@ __global__ void __launch_bounds__(32, 8) batch_fused_warp_kernel(PlanPtrs p) {
 // shared memory once, each warp's ket records too, in two buffers (fsym_tile
 // with BSYNC, SBRA, SKET).  Shared memory is sized for n = kMaxN.
 template <int N> __host__ __device__ constexpr int bfused_warp_smem() {
-    return 2 * Part<N>::size * 32 + 2 * 16 * 33 + 32 + 2 * KetLayout<N>::size;
+    return 2 * Part<N>::size * 32 + 2 * 16 * 33 + 64 + 2 * KetLayout<N>::size;
 }
 constexpr int kBatchFusedSmem = (8 * bfused_warp_smem<kMaxN>() + BraLayout<kMaxN>::size * 32) * 8;
 
@@ -215,7 +215,7 @@ __device__ __forceinline__ void batch_fused_group(const InstDesc &d, int2 gr, do
     double *base = smem + w * PER_WARP;
     double *sbra = smem + 8 * PER_WARP;
     const FusedSmem sm{base, base + 2 * PS * 32, base + 2 * PS * 32 + 2 * 16 * 33,
-                       base + 2 * PS * 32 + 2 * 16 * 33 + 32};
+                       base + 2 * PS * 32 + 2 * 16 * 33 + 64};
     const int K = d.K, kb = gr.x, lc = gr.y + w;
     const int last = min(kb * 32 + 31, K - 1);
     const bool idle = lc * d.lc_s > last;

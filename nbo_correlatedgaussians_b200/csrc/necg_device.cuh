@@ -63,8 +63,8 @@ struct TileOut {
 };
 
 // Shared memory of one warp's fused tile: bra accumulators for H and S
-// (2 * PS * 32 doubles), two ket tables of 16 rows (2 * 16 * 33) and one
-// reduction row (32).  Sized by the caller for its largest n.
+// (2 * PS * 32 doubles), two ket tables of 16 rows (2 * 16 * 33) and two
+// reduction rows (64).  Sized by the caller for its largest n.
 struct FusedSmem {
     double *sacc, *krow, *kred;
     double *sket;  // SKET: two ket-record buffers of this warp (16-byte aligned)
@@ -216,22 +216,33 @@ __device__ __forceinline__ void fsym_tile(int t, int2 tl, int LC, int K, int nst
                 ssum += w * ov;
             }
             __syncwarp();
+            // the 16 rows of both ket tables, summed as trees (four dependent
+            // adds instead of sixteen), then mapped to l's frame together
+            if (lane < PS) {
+                double vh[16], vs[16];
 #pragma unroll
-            for (int which = 0; which < 2; ++which) {
-                const double *kt = which ? krow1 : krow0;
-                double v = 0.0;
-                if (lane < PS)
-#pragma unroll
-                    for (int r = 0; r < 16; ++r) v += kt[r * 33 + lane];
-                kred[lane] = v;
-                __syncwarp();
-                if (lane < PS) {
-                    const double m = ket_map_apply(kmap, P, lane, PS, kred);
-                    if (which == 0) aH += m;
-                    else aS += m;
+                for (int r = 0; r < 16; ++r) {
+                    vh[r] = krow0[r * 33 + lane];
+                    vs[r] = krow1[r * 33 + lane];
                 }
-                __syncwarp();
+#pragma unroll
+                for (int w = 8; w >= 1; w >>= 1)
+#pragma unroll
+                    for (int r = 0; r < w; ++r) {
+                        vh[r] += vh[r + w];
+                        vs[r] += vs[r + w];
+                    }
+                kred[lane] = vh[0];
+                kred[32 + lane] = vs[0];
             }
+            __syncwarp();
+            if (lane < PS) {
+                double mh, ms;
+                ket_map_apply2(kmap, P, lane, PS, kred, kred + 32, mh, ms);
+                aH += mh;
+                aS += ms;
+            }
+            __syncwarp();
             if (BSYNC && sync_at == 0) cta_barrier();
         }
         if (BSYNC && !lok) continue;

@@ -288,7 +288,7 @@ __global__ void __launch_bounds__(32, MINW) fsym_kernel(const int2 *__restrict__
                                                    double *__restrict__ part_k, int *status) {
     __shared__ double sacc[2 * Part<N>::size * 32];
     __shared__ double krow[2 * 16 * 33];
-    __shared__ double kred[32];
+    __shared__ double kred[64];
     __shared__ __align__(16) double sket[SKET ? 2 * KetLayout<N>::size : 2];
     const int t = t_begin + blockIdx.x;
     if (t >= t_end) return;
@@ -323,10 +323,10 @@ __global__ void __launch_bounds__(256) hs_reduce_kernel(const double *__restrict
 // shared memory once for all warps; SKET: each warp stages its ket records in
 // two buffers (the next term's copied while the current one is evaluated).
 // SYNC: where the warps take their per-term barrier (fsym_tile).  Shared
-// memory (dynamic, 16-byte aligned): per warp 2 PS 32 + 2 16 33 + 32 (+ 2 ket
+// memory (dynamic, 16-byte aligned): per warp 2 PS 32 + 2 16 33 + 64 (+ 2 ket
 // records) doubles, then the bras.
 template <int N> __host__ __device__ constexpr int fsym_warp_smem(bool sket) {
-    return 2 * Part<N>::size * 32 + 2 * 16 * 33 + 32 + (sket ? 2 * KetLayout<N>::size : 0);
+    return 2 * Part<N>::size * 32 + 2 * 16 * 33 + 64 + (sket ? 2 * KetLayout<N>::size : 0);
 }
 template <int N> __host__ __device__ constexpr int fsym_block_smem_bytes(int warps, bool sbra, bool sket) {
     return (warps * fsym_warp_smem<N>(sket) + (sbra ? BraLayout<N>::size * 32 : 0)) * 8;
@@ -353,7 +353,7 @@ __global__ void __launch_bounds__(32 * WARPS, 1) fsym_block_kernel(const int2 *_
     double *base = smem + w * PER_WARP;
     double *sbra = smem + WARPS * PER_WARP;  // SBRA: BS x 32 doubles after the warps' areas
     const FusedSmem sm{base, base + 2 * PS * 32, base + 2 * PS * 32 + 2 * 16 * 33,
-                       base + 2 * PS * 32 + 2 * 16 * 33 + 32};
+                       base + 2 * PS * 32 + 2 * 16 * 33 + 64};
     for (;;) {
         if (threadIdx.x == 0) gsh = atomicAdd(qcount, 1);
         __syncthreads();

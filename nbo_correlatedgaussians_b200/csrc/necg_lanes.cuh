@@ -371,6 +371,23 @@ NECG_HD double ket_map_apply(const KetMap &m, int P, int f, int PS, const double
     return v;
 }
 
+// The same map applied to two inputs (the H and S ket gradients), reading the
+// map entries once.
+NECG_HD void ket_map_apply2(const KetMap &m, int P, int f, int PS, const double *in0, const double *in1,
+                            double &out0, double &out1) {
+    const int e = P * PS + f;
+    const int n = m.cnt[e];
+    double v0 = 0.0, v1 = 0.0;
+    for (int i = 0; i < n; ++i) {
+        const double c = m.coef[(size_t)e * m.maxnz + i];
+        const int s = m.src[(size_t)e * m.maxnz + i];
+        v0 += c * in0[s];
+        v1 += c * in1[s];
+    }
+    out0 = v0;
+    out1 = v1;
+}
+
 // Lane ranges of the two tile kinds (used by the kernels and the emulator).
 // Energy: tile (kb, lc) -> bra k = 32 kb + lane, kets [l0, lend); false if idle.
 NECG_HD bool energy_lane_range(int kb, int lc, int lane, int LC, int K, int &k, int &l0, int &lend) {
