@@ -725,10 +725,10 @@ __global__ void f0_kernel(const double *__restrict__ z, int count, double *__res
                           double *__restrict__ df) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= count) return;
-    double fs, dfs, ia, zo;
-    boys<true>(1.0, z[i], fs, dfs, ia, zo);  // a = 1: fs = F0(z), dfs = F0'(z)
+    double fs, D, ia, zo;
+    boys<true>(1.0, z[i], fs, D, ia, zo);  // a = 1: fs = F0(z), D = F0'(z) / F0(z)
     if (f) f[i] = fs;
-    if (df) df[i] = dfs;
+    if (df) df[i] = fs * D;
 }
 
 __global__ void reset_status_kernel(int *status) {

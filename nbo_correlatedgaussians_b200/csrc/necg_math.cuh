@@ -285,18 +285,18 @@ NECG_HD void symv3(const Acc &S, int off, const R (&x)[3 * N], R (&y)[3 * N]) {
 
 // Boys-function pieces for one Coulomb pair.  Given a = v^T Bi v and
 // bb = |v^T T|^2 (z = bb / a) returns fs = F0(z) a^{-1/2} and, when GRAD,
-// dfs = F0'(z) a^{-1/2} and ia = 1/a.  The Pade branch (z <= 16.3578) and the
+// D = F0'(z) / F0(z) (so F0'(z) a^{-1/2} = fs D) and ia = 1/a.  The Pade branch (z <= 16.3578) and the
 // asymptotic branch sqrt(pi/(4z)) follow python/utils.py:78-106; in the Pade
 // branch F0 = sqrt(num / den).  Two reciprocal square roots give every
 // quotient and root needed:
 //   ra = a^{-1/2}:          1/a = ra^2,  fs = F0 ra
 //   q = (num den)^{-1/2}:   F0 = num q,  q^2 = 1 / (num den)
 // and, from F0^2 = num / den, F0' = F0 (num'/num - den'/den) / 2, so
-//   F0' a^{-1/2} = fs q^2 (num' den - den' num) / 2,
+//   D = F0' / F0 = q^2 (num' den - den' num) / 2,
 // with num'/2 and den'/2 evaluated directly (halved coefficients: exact).
 #pragma nv_exec_check_disable
 template <bool GRAD, typename R>
-NECG_HD void boys(R a, R bb, R &fs, R &dfs, R &ia, R &z) {
+NECG_HD void boys(R a, R bb, R &fs, R &D, R &ia, R &z) {
     const R ra = rsq(a);
     ia = ra * ra;
     z = bb * ia;
@@ -313,16 +313,16 @@ NECG_HD void boys(R a, R bb, R &fs, R &dfs, R &ia, R &z) {
                            NECG_PC4) * z + 0.5 * NECG_PC5;
             const R dDh = ((((3.0 * NECG_PC6 * z + 2.5 * NECG_PC7) * z + 2.0 * NECG_PC8) * z +
                             1.5 * NECG_PC9) * z + NECG_PC10) * z + 0.5 * NECG_PC11;
-            dfs = fs * (q * q) * (dNh * den - dDh * num);
+            D = (q * q) * (dNh * den - dDh * num);
         } else {
-            dfs = R(0.0);
+            D = R(0.0);
         }
     } else {
         // F0 = sqrt(pi / (4 z)) ; F0 a^-1/2 = sqrt(pi / (4 bb))
         const R rb = rsq(bb);
         fs = (0.5 * NECG_SQRT_PI) * rb;
-        if (GRAD) dfs = -0.5 * fs * a * rb * rb;  // F0' = -F0 / (2 z)
-        else dfs = R(0.0);
+        if (GRAD) D = -0.5 * a * (rb * rb);  // F0' / F0 = -1 / (2 z)
+        else D = R(0.0);
     }
 }
 
@@ -352,13 +352,14 @@ NECG_HD void coulomb_grad(const R (&Bi)[tri(N)], const R (&T)[3 * N], const Cons
                 for (int c = 0; c < 3; ++c) bv[c] -= T[3 * (p - 1) + c];
             }
             const R bb = bv[0] * bv[0] + bv[1] * bv[1] + bv[2] * bv[2];
-            R fs, dfs, ia, z;
-            boys<true>(a, bb, fs, dfs, ia, z);
-            const double c = cs.cv[vidx(p, q)];
-            rho += c * fs;
-            const R ci = c * ia;
-            const R al = ci * dfs;
-            const R be = ci * (dfs * z + 0.5 * fs);
+            R fs, D, ia, z;
+            boys<true>(a, bb, fs, D, ia, z);
+            // alpha = c F0' a^{-3/2} = c fs D / a, beta = c a^{-3/2} (z F0' + F0 / 2) = (c fs / a)(z D + 1/2)
+            const R cf = cs.cv[vidx(p, q)] * fs;
+            rho += cf;
+            const R cfi = cf * ia;
+            const R al = cfi * D;
+            const R be = cfi * (D * z + 0.5);
 #pragma unroll
             for (int cc = 0; cc < 3; ++cc) Z[3 * (q - 1) + cc] += al * bv[cc];
             W[sx(q - 1, q - 1)] += be;
@@ -535,8 +536,8 @@ NECG_HD bool term_energy(const BA &b, const KA &kr, const Consts<N> &cs, R &ov, 
                 for (int c = 0; c < 3; ++c) bv[c] -= T[3 * (p - 1) + c];
             }
             const R bb = bv[0] * bv[0] + bv[1] * bv[1] + bv[2] * bv[2];
-            R fs, dfs, ia, z;
-            boys<false>(a, bb, fs, dfs, ia, z);
+            R fs, D, ia, z;
+            boys<false>(a, bb, fs, D, ia, z);
             r += cs.cv[vidx(p, q)] * fs;
         }
     rho = r;

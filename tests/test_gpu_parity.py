@@ -368,3 +368,55 @@ def test_symmetric_pass_unavailable_without_inverse_closure(torch_cuda):
     fo, go = Oracle.from_problem(r).outprod(r.x, nthreads=4)
     assert abs(f - fo) < TOL_E and normwise(g, go) < TOL_G
     del keep
+
+
+def _lockstep_tail_parts(K, lc, nst, sms, gw=8):
+    """Parts the host splits each of the lockstep queue's last groups into (the
+    rule of the library's tile builder): G groups, T = G mod SMs of them split
+    into min(4, nst, SMs // T) parts, capped so the units fit the tile slots."""
+    G = tiles = 0
+    for kb in range((K + 31) // 32):
+        t = min(kb * 32 + 31, K - 1) // lc + 1
+        tiles += t
+        G += -(-t // gw)
+    T = G % sms
+    if not T:
+        return 1
+    parts = min(4, nst, sms // T)
+    return min(parts, 1 + (tiles - G) // T)
+
+
+def test_lockstep_queue_tail_split(torch_cuda):
+    """The lockstep pass (variant 258) splits the groups of its queue's last,
+    partial round over the symmetry terms and adds the parts in a fix-up
+    kernel.  At LiH sizes whose tails split 2, 1 (not at all), 4 and 3 ways on a
+    148-SM B200, E, g, H and S must match the one-warp pass (variant 118, which
+    has no queue) to rounding: a lost or doubled part would be an O(1) error."""
+    import torch
+    from nbo_correlatedgaussians_b200 import _lib, synth
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    seen = set()
+    for K in (200, 257, 353, 545):
+        p = synth.make_problem("LiH", K, 60 + K)
+        p.C = np.random.default_rng(K).normal(size=K)
+        eng = _engine(p)
+        res = {}
+        for minw in (118, 258):
+            assert eng.L.necg_set_symmetric(eng.h, 2, 2, minw) == _lib.NECG_OK
+            assert eng.L.necg_set_splits(eng.h, 1) == _lib.NECG_OK
+            H = torch.empty((K, K), dtype=torch.float64, device=eng.device)
+            S = torch.empty_like(H)
+            f, g = eng.outprod_device(torch.from_numpy(p.x), K, H=H, S=S)
+            torch.cuda.synchronize()
+            eng.raise_status("outprod")
+            res[minw] = (float(f.item()), g.cpu().numpy(), H.cpu().numpy(), S.cpu().numpy())
+        eng.close()
+        seen.add(_lockstep_tail_parts(K, 2, p.nst, sms))
+        (f1, g1, H1, S1), (f2, g2, H2, S2) = res[118], res[258]
+        assert abs(f2 - f1) <= 1e-12 * abs(f1), K
+        assert normwise(g2, g1) < 1e-11, K
+        assert np.max(np.abs(H2 - H1)) <= 1e-13 * np.max(np.abs(H1)), K
+        assert np.max(np.abs(S2 - S1)) <= 1e-13 * np.max(np.abs(S1)), K
+        assert np.array_equal(H2, H2.T) and np.array_equal(S2, S2.T)
+    if sms == 148:
+        assert seen == {1, 2, 3, 4}
