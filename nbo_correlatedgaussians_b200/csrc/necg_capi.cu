@@ -120,8 +120,15 @@ template <typename T> int dalloc(necg_handle *h, T **p, size_t count) {
     return NECG_OK;
 }
 
+// Phase event i of the evaluation (profiling).  While the stream is being
+// captured it is recorded as an external event, so that the captured graph
+// records it when it runs.
 void mark(necg_handle *h, int i, cudaStream_t st) {
-    if (h->profile) cudaEventRecord(h->ev[i], st);
+    if (!h->profile) return;
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    cudaStreamIsCapturing(st, &cap);
+    if (cap == cudaStreamCaptureStatusActive) cudaEventRecordWithFlags(h->ev[i], st, cudaEventRecordExternal);
+    else cudaEventRecord(h->ev[i], st);
 }
 
 void free_all(necg_handle *h) {
@@ -153,6 +160,7 @@ int ensure_tiles(necg_handle *h, int K, cudaStream_t st) {
     CK(cudaMemcpyAsync(h->d_tiles, t.data(), t.size() * sizeof(int2), cudaMemcpyHostToDevice, st));
     CK(cudaStreamSynchronize(st));
     h->tiles_K = K;
+    ++h->gversion;  // buffers and lists a captured graph may hold changed
     h->tiles_lc = h->lc_e;
     h->ntiles = (int)t.size();
     return NECG_OK;
@@ -175,6 +183,7 @@ int ensure_sym_tiles(necg_handle *h, int K, cudaStream_t st, int mult) {
         h->hp_cap = 0;
         CK(pool_alloc(h, &h->d_Hp, hp_need * sizeof(double), st));
         CK(pool_alloc(h, &h->d_Sp, hp_need * sizeof(double), st));
+        ++h->gversion;
         h->ws_bytes += (long long)(2 * hp_need * sizeof(double));
         h->hp_cap = hp_need;
     }
@@ -291,6 +300,7 @@ int ensure_sym_tiles(necg_handle *h, int K, cudaStream_t st, int mult) {
     CK(cudaMemcpyAsync(h->d_stile_start, start.data(), start.size() * sizeof(int), cudaMemcpyHostToDevice, st));
     CK(cudaStreamSynchronize(st));
     h->stiles_K = K;
+    ++h->gversion;
     h->stiles_lc = LC;
     h->nstiles = (int)t.size();
     return NECG_OK;
@@ -473,6 +483,52 @@ int finish_launch() {
     return cuda_fail(e);
 }
 
+// The fused evaluation's launch sequence, from the status reset to the
+// partial sums, enqueued on st (no host synchronisation, so it can be captured).
+int enqueue_fused(necg_handle *h, LaunchArgs &a, double *f_dev, double *g_dev, size_t siv, cudaStream_t st) {
+    necg::launch_reset_status(h->d_status, st);
+    mark(h, 0, st);
+    if (necg::launch_prep(a, st)) return NECG_ERR_UNSUPPORTED;
+    mark(h, 1, st);
+    if (necg::launch_fsym(a, st)) return NECG_ERR_ARG;
+    if (necg::launch_fsym_tail(a, st)) return NECG_ERR_ARG;
+    if (necg::launch_hs_reduce(a, st)) return NECG_ERR_ARG;
+    mark(h, 2, st);
+    necg::launch_rows_finalize(a, f_dev, g_dev + siv, 0, 0.0, 0.0, st);
+    mark(h, 3, st);
+    mark(h, 4, st);
+    if (necg::launch_fsym_reduce(a, st)) return NECG_ERR_ARG;
+    mark(h, 5, st);
+    return NECG_OK;
+}
+
+// Capture the fused launch sequence on the handle's own stream and keep it as
+// the handle's graph for `key`.  On any failure the handle keeps no graph for
+// the key and the caller launches eagerly.
+void capture_fused(necg_handle *h, LaunchArgs &a, double *f_dev, double *g_dev, size_t siv,
+                   const necg_handle::GraphKey &key) {
+    if (!h->gstream && cudaStreamCreateWithFlags(&h->gstream, cudaStreamNonBlocking) != cudaSuccess) {
+        h->gstream = nullptr;
+        cudaGetLastError();
+        return;
+    }
+    cudaGraph_t graph = nullptr;
+    if (cudaStreamBeginCapture(h->gstream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        cudaGetLastError();
+        return;
+    }
+    const int rc = enqueue_fused(h, a, f_dev, g_dev, siv, h->gstream);
+    const cudaError_t e = cudaStreamEndCapture(h->gstream, &graph);
+    cudaGraphExec_t exec = nullptr;
+    const bool ok = rc == NECG_OK && e == cudaSuccess && graph && cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;
+    if (graph) cudaGraphDestroy(graph);
+    cudaGetLastError();
+    if (!ok) return;
+    if (h->gexec) cudaGraphExecDestroy(h->gexec);
+    h->gexec = exec;
+    h->gkey = key;
+}
+
 }  // namespace
 
 extern "C" {
@@ -538,6 +594,8 @@ int necg_destroy(necg_handle *h) {
     cudaSetDevice(h->device);
     free_all(h);
     if (h->h_tail) cudaFreeHost(h->h_tail);
+    if (h->gexec) cudaGraphExecDestroy(h->gexec);
+    if (h->gstream) cudaStreamDestroy(h->gstream);
     delete h;
     return NECG_OK;
 }
@@ -549,6 +607,7 @@ int necg_set_tiles(necg_handle *h, int lc_energy, int lc_grad) {
         return NECG_ERR_ARG;
     h->lc_e = lc_energy;
     h->lc_g = lc_grad;
+    ++h->gversion;
     return NECG_OK;
 }
 
@@ -563,12 +622,14 @@ int necg_set_symmetric(necg_handle *h, int mode, int lc, int minw) {
     h->grad_mode = mode;
     h->lc_s = lc;
     h->minb_s = minw;
+    ++h->gversion;
     return NECG_OK;
 }
 
 int necg_set_splits(necg_handle *h, int npc) {
     if (!h || npc < 1 || npc > h->nst) return NECG_ERR_ARG;
     h->npc = npc;
+    ++h->gversion;
     return NECG_OK;
 }
 
@@ -578,6 +639,7 @@ int necg_set_variant(necg_handle *h, int minw_energy, int minw_grad) {
         return NECG_ERR_ARG;
     h->minb_e = minw_energy;
     h->minb_g = minw_grad;
+    ++h->gversion;
     return NECG_OK;
 }
 
@@ -610,7 +672,13 @@ int necg_outprod(necg_handle *h, int K, const double *x_dev, double *f_dev, doub
     if (rc) return rc;
     if (!x_dev || !g_dev) return NECG_ERR_ARG;
     cudaStream_t st = (cudaStream_t)stream;
-    if ((rc = begin(h, st))) return rc;
+    const bool fused = h->grad_mode == 2;
+    if (fused) {  // the status reset is part of the fused launch sequence
+        CK(cudaSetDevice(h->device));
+        h->last_stream = st;
+    } else if ((rc = begin(h, st))) {
+        return rc;
+    }
     if ((rc = ensure_tiles(h, K, st))) return rc;
     const size_t siv = (size_t)K * (h->n * (h->n + 1) / 2 + 3 * h->n);
     LaunchArgs a = base_args(h, K);
@@ -620,7 +688,7 @@ int necg_outprod(necg_handle *h, int K, const double *x_dev, double *f_dev, doub
     a.S = S_dev ? S_dev : h->d_S;
     a.g = g_dev;
     if (h->grad_mode >= 1 && (rc = ensure_sym_tiles(h, K, st, h->grad_mode == 2 ? 2 : 1))) return rc;
-    if (h->grad_mode == 2) {
+    if (fused) {
         // fused: one pass over unordered pairs writes H, S and the split gradients
         a.stiles = h->d_stiles;
         a.stile_start = h->d_stile_start;
@@ -638,18 +706,22 @@ int necg_outprod(necg_handle *h, int K, const double *x_dev, double *f_dev, doub
         a.sg_ntail = h->sg_ntail;
         a.sg_parts = h->sg_parts;
         a.urange = h->d_urange;
-        mark(h, 0, st);
-        if (necg::launch_prep(a, st)) return NECG_ERR_UNSUPPORTED;
-        mark(h, 1, st);
-        if (necg::launch_fsym(a, st)) return NECG_ERR_ARG;
-        if (necg::launch_fsym_tail(a, st)) return NECG_ERR_ARG;
-        if (necg::launch_hs_reduce(a, st)) return NECG_ERR_ARG;
-        mark(h, 2, st);
-        necg::launch_rows_finalize(a, f_dev, g_dev + siv, 0, 0.0, 0.0, st);
-        mark(h, 3, st);
-        mark(h, 4, st);
-        if (necg::launch_fsym_reduce(a, st)) return NECG_ERR_ARG;
-        mark(h, 5, st);
+        // A call that repeats the previous call's buffers, K and settings
+        // replays the captured launch sequence (captured the second time the
+        // same key is seen, so callers whose buffers change every call stay
+        // eager); a stream that is itself being captured gets the launches.
+        cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+        CK(cudaStreamIsCapturing(st, &cap));
+        const necg_handle::GraphKey key{K, x_dev, f_dev, g_dev, a.H, a.S, h->gversion};
+        if (cap == cudaStreamCaptureStatusNone) {
+            if (!(h->gexec && h->gkey == key) && h->gseen == key) capture_fused(h, a, f_dev, g_dev, siv, key);
+            if (h->gexec && h->gkey == key) {
+                CK(cudaGraphLaunch(h->gexec, st));
+                return finish_launch();
+            }
+        }
+        h->gseen = key;
+        if ((rc = enqueue_fused(h, a, f_dev, g_dev, siv, st))) return rc;
         return finish_launch();
     }
     mark(h, 0, st);
@@ -910,6 +982,7 @@ int necg_profile(necg_handle *h, int enable) {
     if (enable && !h->ev[0])
         for (cudaEvent_t &e : h->ev) CK(cudaEventCreate(&e));
     h->profile = enable != 0;
+    ++h->gversion;
     return NECG_OK;
 }
 

@@ -56,6 +56,21 @@ struct necg_handle {
     size_t hp_cap = 0;                        // doubles per buffer
     // pinned host landing area of the host entry point: f, then the two status words
     double *h_tail = nullptr;
+    // the fused evaluation's launch sequence as a CUDA graph: captured (on the
+    // handle's own stream) the second time a call repeats the same key, then
+    // replayed on the caller's stream while the key stays the same
+    struct GraphKey {
+        int K = -1;
+        const void *x = nullptr, *f = nullptr, *g = nullptr, *H = nullptr, *S = nullptr;
+        int version = -1;
+        bool operator==(const GraphKey &o) const {
+            return K == o.K && x == o.x && f == o.f && g == o.g && H == o.H && S == o.S && version == o.version;
+        }
+    };
+    int gversion = 0;  // bumped by every change of settings, tiles or buffers
+    GraphKey gkey, gseen;
+    cudaGraphExec_t gexec = nullptr;
+    cudaStream_t gstream = nullptr;
 };
 
 namespace necg {

@@ -420,3 +420,55 @@ def test_lockstep_queue_tail_split(torch_cuda):
         assert np.array_equal(H2, H2.T) and np.array_equal(S2, S2.T)
     if sms == 148:
         assert seen == {1, 2, 3, 4}
+
+
+@pytest.mark.parametrize("minw,npc", [(258, 1), (118, 4)])
+def test_fused_graph_replay(torch_cuda, minw, npc):
+    """A call that repeats the previous call's buffers, K and settings replays
+    the fused pass's launch sequence as a captured CUDA graph (from the third
+    such call on).  Its results must be bitwise those of eager launches, it must
+    read new contents of the same x buffer, and a settings change must leave it."""
+    import torch
+    from nbo_correlatedgaussians_b200 import _lib, synth
+    p = synth.make_problem("LiH", 40, 11)
+    p.C = np.random.default_rng(3).normal(size=40)
+    eng = _engine(p)
+    L = eng.L
+    assert L.necg_set_symmetric(eng.h, 2, 2, minw) == _lib.NECG_OK
+    assert L.necg_set_splits(eng.h, npc) == _lib.NECG_OK
+    x = torch.from_numpy(p.x).cuda()
+    g = torch.empty_like(x)
+    f = torch.empty(1, dtype=torch.float64, device="cuda")
+    outs = []
+    for _ in range(5):  # eager, eager + capture, then replays
+        eng.outprod_device(x, p.K, g=g, f=f)
+        torch.cuda.synchronize()
+        eng.raise_status("outprod")
+        outs.append((float(f.item()), g.cpu().numpy().copy()))
+    for fo, go in outs[1:]:
+        assert fo == outs[0][0] and np.array_equal(go, outs[0][1])
+    fr, gr = Oracle.from_problem(p).outprod(p.x, nthreads=8)
+    assert abs(outs[0][0] - fr) < TOL_E and normwise(outs[0][1], gr) < TOL_G
+    # new contents in the same buffer: the replay reads them
+    q = p.copy()
+    q.iv = q.iv * 1.01
+    x.copy_(torch.from_numpy(q.x))
+    eng.outprod_device(x, p.K, g=g, f=f)
+    torch.cuda.synchronize()
+    f2, g2 = float(f.item()), g.cpu().numpy().copy()
+    fe, ge = eng.outprod_device(torch.from_numpy(q.x).cuda(), p.K)  # other buffers: eager
+    torch.cuda.synchronize()
+    assert f2 == float(fe.item()) and np.array_equal(g2, ge.cpu().numpy())
+    # a non-positive-definite input through the replay, then a good one
+    bad = p.copy()
+    bad.iv[2 * p.blk:2 * p.blk + p.svh] = 0.0
+    x.copy_(torch.from_numpy(bad.x))
+    eng.outprod_device(x, p.K, g=g, f=f)
+    with pytest.raises(np.linalg.LinAlgError):
+        eng.raise_status("outprod")
+    x.copy_(torch.from_numpy(p.x))
+    eng.outprod_device(x, p.K, g=g, f=f)
+    torch.cuda.synchronize()
+    eng.raise_status("outprod")
+    assert float(f.item()) == outs[0][0] and np.array_equal(g.cpu().numpy(), outs[0][1])
+    eng.close()
