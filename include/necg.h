@@ -112,7 +112,12 @@ int necg_set_splits(necg_handle *h, int npc);
 /* One objective evaluation: python/outprod.py:20-76 outprod(x) -> (f, g),
  * including make_grad (python/make_grad.py:18-90).  Device pointers; H_dev and
  * S_dev (K*K) receive the symmetric matrices and may be NULL (workspace is used).
- * Asynchronous on `stream`; the pair status is read by necg_status(). */
+ * Asynchronous on `stream`; the pair status is read by necg_status().  With the
+ * fused pass, a call that repeats the previous call's pointers, K and settings
+ * launches the evaluation as one CUDA graph (captured on the handle's own stream
+ * the second time the same call is seen); results are bitwise those of the
+ * separate launches.  While `stream` is itself being captured, the kernels are
+ * launched into that capture instead. */
 int necg_outprod(necg_handle *h, int K, const double *x_dev, double *f_dev, double *g_dev,
                  double *H_dev, double *S_dev, void *stream);
 
