@@ -222,15 +222,16 @@ int ensure_sym_tiles(necg_handle *h, int K, cudaStream_t st, int mult) {
     // The groups are equal work, one block per SM takes them from the queue, so
     // the last round runs G mod SMs groups while the other SMs idle: split each
     // of those groups into `parts` units over the symmetry terms (as many as
-    // keep the round within one unit per SM, at most 4), so the last round is a
-    // part of a group long.
+    // keep the round within one unit per SM, at most 8; the kernel gives the
+    // parts balanced ranges of terms), so the last round is a part of a group
+    // long.
     {
         int sms = 148;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device);
         const int G = (int)groups.size();
         const int T = G % sms;
         int parts = T > 0 ? sms / T : 1;
-        if (parts > 4) parts = 4;
+        if (parts > 8) parts = 8;
         if (parts > h->nst) parts = h->nst;
         // the lockstep pass writes bra partials per queue unit into the slots
         // sized for the tiles: G - T + T parts units must not exceed them

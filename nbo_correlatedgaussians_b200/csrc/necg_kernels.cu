@@ -367,7 +367,7 @@ __global__ void __launch_bounds__(32 * WARPS, 1) fsym_block_kernel(const int2 *_
         // a split group of the queue's tail: this unit takes symmetry terms
         // [p0, p1); parts after the first write to their own slots in xsym
         const int part = sgroup_part(gr), parts = sgroup_parts(gr);
-        const int PC = (nst + parts - 1) / parts, p0 = min(part * PC, nst), p1 = min(p0 + PC, nst);
+        const int p0 = part * nst / parts, p1 = (part + 1) * nst / parts;  // balanced ranges
         TileOut xo;
         if (part > 0) {
             xo.x = xsym;
