@@ -441,10 +441,10 @@ __global__ void __launch_bounds__(256) fsym_tail_fix_kernel(const int2 *__restri
 // Sum the fused-pass partials and combine out[f * K + m] = sum_H - E sum_S with
 // E = scal[0] (written by finalize after the pass).  Block (kb, f): the 32
 // bases of row block kb, field f.  Their bra partials come from every tile of
-// block kb (up to K / LC of them), so the 8 warps of the block take every 8th
-// tile and their sums are combined in a fixed order; the ket partials (one
-// tile per later row block) are added by the first warp.  Only tiles in
-// [t0, t1) count (a shard of the pass).
+// block kb (up to K / LC of them) and their ket partials from one tile per
+// later row block, so the 8 warps of the block take every 8th of each and
+// their sums are combined in a fixed order.  Only tiles in [t0, t1) count (a
+// shard of the pass).
 template <int N>
 __global__ void __launch_bounds__(256) fsym_sum_kernel(const int *__restrict__ tstart, int LC, int K,
                                                        const double *__restrict__ part_b,
@@ -453,7 +453,7 @@ __global__ void __launch_bounds__(256) fsym_sum_kernel(const int *__restrict__ t
                                                        double *__restrict__ out, int t0, int t1, int npc,
                                                        const int2 *__restrict__ urange) {
     constexpr int PS = Part<N>::size;
-    __shared__ double red[2][8][32];
+    __shared__ double red[4][8][32];
     const int kb = blockIdx.x, f = blockIdx.y;
     const int lane = threadIdx.x & 31, seg = threadIdx.x >> 5;
     const int m = kb * 32 + lane;
@@ -466,10 +466,31 @@ __global__ void __launch_bounds__(256) fsym_sum_kernel(const int *__restrict__ t
         sH += part_b[(((size_t)t * 2 + 0) * PS + f) * 32 + lane];
         sS += part_b[(((size_t)t * 2 + 1) * PS + f) * 32 + lane];
     }
+    // the ket partials of basis m: tile (q, lc) of every row block q from
+    // kb0 on, every 8th q per warp
+    double kH = 0.0, kS = 0.0;
+    if (m < K) {
+        const int lc = m / LC, ll = m - lc * LC;
+        const int nkb = (K + 31) >> 5;
+        int kb0 = lc * LC - 31;
+        kb0 = kb0 > 0 ? (kb0 + 31) >> 5 : 0;
+        for (int q = kb0 + seg; q < nkb; q += 8) {
+            const int t = tstart[q] + lc;
+            if (t < t0 || t >= t1) continue;
+            for (int pc = 0; pc < npc; ++pc) {
+                const size_t base = ((size_t)(t * npc + pc) * LC + ll) * 2;
+                kH += part_k[(base + 0) * PS + f];
+                kS += part_k[(base + 1) * PS + f];
+            }
+        }
+    }
     red[0][seg][lane] = sH;
     red[1][seg][lane] = sS;
+    red[2][seg][lane] = kH;
+    red[3][seg][lane] = kS;
     __syncthreads();
     if (seg != 0 || m >= K) return;
+    // fixed order: the bra sums of the 8 warps, then their ket sums
     sH = red[0][0][lane];
     sS = red[1][0][lane];
 #pragma unroll
@@ -477,18 +498,10 @@ __global__ void __launch_bounds__(256) fsym_sum_kernel(const int *__restrict__ t
         sH += red[0][q][lane];
         sS += red[1][q][lane];
     }
-    const int lc = m / LC, ll = m - lc * LC;
-    const int nkb = (K + 31) >> 5;
-    int kb0 = lc * LC - 31;
-    kb0 = kb0 > 0 ? (kb0 + 31) >> 5 : 0;
-    for (int q = kb0; q < nkb; ++q) {
-        const int t = tstart[q] + lc;
-        if (t < t0 || t >= t1) continue;
-        for (int pc = 0; pc < npc; ++pc) {
-            const size_t base = ((size_t)(t * npc + pc) * LC + ll) * 2;
-            sH += part_k[(base + 0) * PS + f];
-            sS += part_k[(base + 1) * PS + f];
-        }
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        sH += red[2][q][lane];
+        sS += red[3][q][lane];
     }
     out[(size_t)f * K + m] = sH - scal[0] * sS;
 }

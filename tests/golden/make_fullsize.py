@@ -19,7 +19,12 @@ SHA-256 of the x it was made from so a test can tell that it has the same x):
                           and 8192 sampled H and S entries.
   fullsize_lih_k731.npz   the largest LiH instance of the 64-instance mixed
                           batch (K=731, seed 3000 + index): f and g at C = 1/K.
-The oracle runs on every host core; the whole set takes a few minutes.
+  fullsize_serve_lih.npz, fullsize_serve_he.npz
+                          the largest LiH run (K=1928) and the largest He run
+                          (K=2032) of the 256-run serving stream: f and g at
+                          C = 1/K.
+The oracle runs on every host core; the whole set takes about half an hour on
+8 cores (most of it the LiH K=1928 run).
 """
 from __future__ import annotations
 
@@ -103,7 +108,22 @@ def gen_lih_k731():
                         n=p.n, x_sum=float(x.sum()), x_sha=x_digest(x), f=f, g=g)
 
 
-GENERATORS = {"lih_k1024": gen_lih_k1024, "h2_k2048": gen_h2_k2048, "lih_k731": gen_lih_k731}
+def largest_serve_run(n: int):
+    """(index, Problem) of the largest run with n particles in the 256-run serving stream."""
+    runs = synth.workload("serve256")
+    j = max((i for i, q in enumerate(runs) if q.n == n), key=lambda i: runs[i].K)
+    return j, runs[j]
+
+
+def gen_serve(n: int, tag: str):
+    j, p = largest_serve_run(n)
+    x, (f, g) = evaluate(p)
+    np.savez_compressed(os.path.join(HERE, f"fullsize_serve_{tag}.npz"), workload="serve256", index=j, K=p.K,
+                        n=p.n, x_sum=float(x.sum()), x_sha=x_digest(x), f=f, g=g)
+
+
+GENERATORS = {"lih_k1024": gen_lih_k1024, "h2_k2048": gen_h2_k2048, "lih_k731": gen_lih_k731,
+              "serve_he": lambda: gen_serve(2, "he"), "serve_lih": lambda: gen_serve(5, "lih")}
 
 if __name__ == "__main__":
     for name in sys.argv[1:] or list(GENERATORS):

@@ -6,6 +6,8 @@ against oracle fixtures made by tests/golden/make_fullsize.py.
   H2 n=3, K=2048, nst=4, seed 2     C = 1/K; tuned and ordered passes
   LiH K=731 (largest LiH instance   per call and inside the 64-instance
   of the mixed batch)               batched step
+  the largest LiH (K=1928) and He   per call and together in one batched step
+  (K=2032) runs of the serving stream
 
 Tolerances (the reference's own quantities, python/outprod.py:20-76 and
 python/make_grad.py:18-90): E within 1e-10 Eh absolute; g within 1e-9
@@ -160,3 +162,38 @@ def test_mixed_batch_largest_lih():
           f"batched: |dE|={dE2:.2e} Eh g={dg2:.2e}")
     assert dE1 < TOL_E and dg1 < TOL_G
     assert dE2 < TOL_E and dg2 < TOL_G
+
+
+def test_serving_stream_largest_runs():
+    """The largest LiH run (K=1928) and the largest He run (K=2032) of the
+    256-run serving stream, per call with the tuned pass and together in one
+    batched step (the step the serving loop runs)."""
+    import torch
+    from nbo_correlatedgaussians_b200 import synth
+    from nbo_correlatedgaussians_b200.batch import BatchEngine
+    from nbo_correlatedgaussians_b200.engine import Engine
+    runs = synth.workload("serve256")
+    fixtures = [golden("fullsize_serve_lih.npz"), golden("fullsize_serve_he.npz")]
+    probs = []
+    for d in fixtures:
+        p = runs[int(d["index"])]
+        assert p.K == int(d["K"]) and _sha(p.x) == str(d["x_sha"])
+        probs.append(p)
+        eng = Engine(p)
+        _set_pass(eng, "tuned", p.x, p.K)
+        f, g = _eval(eng, p.x, p.K, with_hs=False)
+        eng.close()
+        dE, dg = abs(f - float(d["f"])), normwise(g, d["g"])
+        print(f"PARITY serve256 run {int(d['index'])} (n={p.n}, K={p.K}) per call: |dE|={dE:.2e} Eh g={dg:.2e}")
+        assert dE < TOL_E and dg < TOL_G
+    be = BatchEngine(probs, tune=True)
+    be.plan()
+    be.step()
+    torch.cuda.synchronize()
+    be.check()
+    for i, d in enumerate(fixtures):
+        f, g = be.results(i)
+        dE, dg = abs(f - float(d["f"])), normwise(g, d["g"])
+        print(f"PARITY serve256 run {int(d['index'])} batched: |dE|={dE:.2e} Eh g={dg:.2e}")
+        assert dE < TOL_E and dg < TOL_G
+    be.close()
