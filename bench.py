@@ -78,7 +78,7 @@ def parse():
     return ap.parse_args()
 
 
-DEFAULT_TILES = {"lc_e": 2, "minb_e": 16, "lc_g": 4, "minb_g": 8, "sym": 2, "lc_s": 2, "minw_s": 258}
+DEFAULT_TILES = {"lc_e": 2, "minb_e": 16, "lc_g": 4, "minb_g": 8, "sym": 2, "lc_s": 2, "minw_s": 248}
 PASS_MODE = {"ordered": 0, "symmetric": 1, "fused": 2}
 # FP64 FLOPs per (k, l, P) term (FMA = 2; each div/sqrt/rsqrt/exp = 1), frozen at
 # the counts the kernels' own templates gave when the fused pass was first

@@ -43,7 +43,7 @@ template <int N> void host_records(std::vector<double> &bra, std::vector<double>
         ket[KL::Sp + t] = -0.01 * (t + 2);
         ket[KL::ASp + t] = -0.015 * (t + 2);
     }
-    for (int t = 0; t < N * N; ++t) ket[KL::AMp + t] = 0.01 * t;
+    for (int t = 0; t < N * N; ++t) ket[KL::AMn4 + t] = -0.04 * t;
     bra[BL::i1] = 0.01;
     bra[BL::pre] = 1.0;
     bra[BL::tMA] = 2.0;
@@ -64,12 +64,27 @@ struct CountRow {
         ++count_ctx().flops;
     }
 };
+// The fused pass's ket output: the H and S values of one field together.
+struct CountRow2 {
+    CountRow h, s;
+    void put(int f, CD vh, CD vs) {
+        h.put(f, vh);
+        s.put(f, vs);
+    }
+    void add(int f, CD vh, CD vs) {
+        h.add(f, vh);
+        s.add(f, vs);
+    }
+};
 
 template <int N> void count_term(int which, long long &flops, long long &special) {
     std::vector<double> bra, ket;
     host_records<N>(bra, ket);
     Consts<N> cs;
-    for (int i = 0; i < N * N; ++i) cs.M[i] = (i % (N + 1) == 0) ? 0.5 : 0.01;
+    for (int i = 0; i < N * N; ++i) {
+        cs.M[i] = (i % (N + 1) == 0) ? 0.5 : 0.01;
+        cs.M4[i] = 4.0 * cs.M[i];
+    }
     for (int t = 0; t < tri(N); ++t) cs.cv[t] = 1.0;
     for (int i = 0; i < N; ++i) cs.q[i] = -1.0;
     cs.efs = 1e-4;
@@ -101,10 +116,10 @@ template <int N> void count_term(int which, long long &flops, long long &special
         RegAcc<N, CD> aH, aS;
         aH.zero();
         aS.zero();
-        CountRow kH, kS;
+        CountRow2 ko;
         count_ctx() = CountCtx();
         CD h, ov, hs(0.0), ss(0.0), w(1.0);
-        term_fused<N>(b, kr, cs, CD(1.0), CD(1.0), aH, aS, kH, kS, h, ov);
+        term_fused<N>(b, kr, cs, CD(1.0), CD(1.0), aH, aS, ko, h, ov);
         hs += w * h;  // the pass's sums of w_P h and w_P ov over P
         ss += w * ov;
     }

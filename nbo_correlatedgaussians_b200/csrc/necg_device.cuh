@@ -132,19 +132,19 @@ __device__ __forceinline__ void fsym_tile(int t, int2 tl, int LC, int K, int nst
     SmemAcc<N> accH{sm.sacc + lane}, accS{sm.sacc + PS * 32 + lane};
     accH.zero();
     accS.zero();
-    // ket row output: lanes 2i and 2i+1 add their values; lane 2i writes row i
+    // ket row output: lanes 2i and 2i+1 add their values of field f with one
+    // exchange, lane 2i the H values (into row i of the H table), lane 2i+1 the
+    // S values (row i of the S table)
     struct PairOut {
         double *r;
-        bool lead;
-        __device__ __forceinline__ void put(int f, double v) {
-            v += __shfl_xor_sync(0xffffffffu, v, 1);
-            if (lead) r[f] = v;
+        bool odd;
+        __device__ __forceinline__ double sum(double vh, double vs) const {
+            const double keep = odd ? vs : vh;
+            return keep + __shfl_xor_sync(0xffffffffu, odd ? vh : vs, 1);
         }
-        __device__ __forceinline__ void add(int f, double v) {
-            v += __shfl_xor_sync(0xffffffffu, v, 1);
-            if (lead) r[f] += v;
-        }
-    } koH{krow0 + (lane >> 1) * 33, !(lane & 1)}, koS{krow1 + (lane >> 1) * 33, !(lane & 1)};
+        __device__ __forceinline__ void put(int f, double vh, double vs) { r[f] = sum(vh, vs); }
+        __device__ __forceinline__ void add(int f, double vh, double vs) { r[f] += sum(vh, vs); }
+    } ko{((lane & 1) ? krow1 : krow0) + (lane >> 1) * 33, (lane & 1) != 0};
     bool ok = true;
     int flags = 0, bad = 0x7fffffff;  // smallest failing pair (row-major k K + l)
     // where this warp takes its per-term block barrier (BSYNC): 0 at the end of
@@ -195,17 +195,17 @@ __device__ __forceinline__ void fsym_tile(int t, int2 tl, int LC, int K, int nst
             double h, ov;
             bool tok;
             if constexpr (SBRA && SKET)
-                tok = term_fused<N, double>(BraSmem{sbra + lane}, KetSmem{kr}, cs, wb, wk, accH, accS, koH, koS, h,
-                                            ov, mid);
+                tok = term_fused<N, double>(BraSmem{sbra + lane}, KetSmem{kr}, cs, wb, wk, accH, accS, ko, h, ov,
+                                            mid);
             else if constexpr (SBRA)
-                tok = term_fused<N, double>(BraSmem{sbra + lane}, KetRefV{kr}, cs, wb, wk, accH, accS, koH, koS, h,
-                                            ov, mid);
+                tok = term_fused<N, double>(BraSmem{sbra + lane}, KetRefV{kr}, cs, wb, wk, accH, accS, ko, h, ov,
+                                            mid);
             else if constexpr (SKET)
-                tok = term_fused<N, double>(b, KetSmem{kr}, cs, wb, wk, accH, accS, koH, koS, h, ov);
+                tok = term_fused<N, double>(b, KetSmem{kr}, cs, wb, wk, accH, accS, ko, h, ov);
             else if constexpr (VKET)
-                tok = term_fused<N, double>(b, KetRefV{kr}, cs, wb, wk, accH, accS, koH, koS, h, ov);
+                tok = term_fused<N, double>(b, KetRefV{kr}, cs, wb, wk, accH, accS, ko, h, ov);
             else
-                tok = term_fused<N, double>(b, kr, cs, wb, wk, accH, accS, koH, koS, h, ov);
+                tok = term_fused<N, double>(b, kr, cs, wb, wk, accH, accS, ko, h, ov);
             if (active) {
                 if (!tok && ok) {  // the first pair of this lane that is not positive definite
                     ok = false;

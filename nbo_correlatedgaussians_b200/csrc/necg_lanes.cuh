@@ -157,7 +157,7 @@ NECG_HD void prep_ket_one(const double *iv, const double *C, int nst, const Cons
 #pragma unroll
     for (int t = 0; t < tri(N); ++t) o[KL::Np + t] = AMA[t];
 #pragma unroll
-    for (int t = 0; t < N * N; ++t) o[KL::AMp + t] = AM[t];
+    for (int t = 0; t < N * N; ++t) o[KL::AMn4 + t] = -4.0 * AM[t];
     o[KL::i2] = i2;
     o[KL::pre] = dl * ::sqrt(dl);
     o[KL::tMA] = tMA;

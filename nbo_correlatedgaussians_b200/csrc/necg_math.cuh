@@ -72,15 +72,17 @@ __host__ __device__ constexpr int sx(int i, int j) {
 #define NECG_SQRT_PI 1.7724538509055159
 
 // Ket record: one per (l, P), read warp-uniformly by the tile kernels.
-// Layout (doubles): Ap[tri] Sp[3N] ASp[3N] Np[tri] AMp[N*N] i2 pre tMA w wC winv pad
+// Layout (doubles): Ap[tri] Sp[3N] ASp[3N] Np[tri] AMn4[N*N] i2 pre tMA w wC winv pad
+// (AMn4 = -4 A_l' M, row-major: the factor of Z's update folded in, so that the
+// update is one FMA chain per output)
 template <int N> struct KetLayout {
     static constexpr int T = tri(N);
     static constexpr int Ap = 0;
     static constexpr int Sp = Ap + T;
     static constexpr int ASp = Sp + 3 * N;
     static constexpr int Np = ASp + 3 * N;
-    static constexpr int AMp = Np + T;
-    static constexpr int i2 = AMp + N * N;
+    static constexpr int AMn4 = Np + T;
+    static constexpr int i2 = AMn4 + N * N;
     static constexpr int pre = i2 + 1;
     static constexpr int tMA = pre + 1;  // tr(M A_l')
     static constexpr int w = tMA + 1;    // symmetry weight scvv[P]
@@ -106,6 +108,7 @@ template <int N> struct BraLayout {
 // Per-problem constants, passed to kernels by value (constant bank).
 template <int N> struct Consts {
     double M[N * N];    // inverse-mass tensor, row-major
+    double M4[N * N];   // 4 M (Q_l = Q_k + 4 M Y as one FMA chain per output)
     double cv[tri(N)];  // c_v for the n(n+1)/2 Coulomb pairs (p<q, q-major order)
     double q[N];        // ncv[1..n]
     double efs;
@@ -602,10 +605,10 @@ NECG_HD bool term_grad(const BA &b, const KA &kr, const Consts<N> &cs, R lam, R 
     for (int i = 0; i < N; ++i)
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-            R s = kr[KL::AMp + i * N] * Y[c];
+            R s = Z[3 * i + c];
 #pragma unroll
-            for (int k = 1; k < N; ++k) s += kr[KL::AMp + i * N + k] * Y[3 * k + c];
-            Z[3 * i + c] -= 4.0 * s;
+            for (int k = 0; k < N; ++k) s += kr[KL::AMn4 + i * N + k] * Y[3 * k + c];
+            Z[3 * i + c] = s;
         }
     R Q[3 * N];
 #pragma unroll
@@ -703,10 +706,10 @@ NECG_HD bool term_sym(const BA &b, const KA &kr, const Consts<N> &cs, R E, R wb,
     for (int i = 0; i < N; ++i)
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-            R s = kr[KL::AMp + i * N] * Y[c];
+            R s = Z[3 * i + c];
 #pragma unroll
-            for (int k = 1; k < N; ++k) s += kr[KL::AMp + i * N + k] * Y[3 * k + c];
-            Z[3 * i + c] -= 4.0 * s;
+            for (int k = 0; k < N; ++k) s += kr[KL::AMn4 + i * N + k] * Y[3 * k + c];
+            Z[3 * i + c] = s;
         }
     R Qk[3 * N], Ql[3 * N];
 #pragma unroll
@@ -722,10 +725,10 @@ NECG_HD bool term_sym(const BA &b, const KA &kr, const Consts<N> &cs, R E, R wb,
     for (int i = 0; i < N; ++i)
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-            R s = cs.M[i * N] * Y[c];
+            R s = Qk[3 * i + c];
 #pragma unroll
-            for (int k = 1; k < N; ++k) s += cs.M[i * N + k] * Y[3 * k + c];
-            Ql[3 * i + c] = Qk[3 * i + c] + 4.0 * s;
+            for (int k = 0; k < N; ++k) s += cs.M4[i * N + k] * Y[3 * k + c];
+            Ql[3 * i + c] = s;
         }
     // bra: acc.s += 2 ovb A_k Qk - 2 Fb Y ; ket: put 2 ovk A_l' Ql + 2 Fk Y
     {
@@ -780,7 +783,8 @@ NECG_HD bool term_sym(const BA &b, const KA &kr, const Consts<N> &cs, R E, R wb,
 // Fb = wb h, ovb = wb ov (Fk, ovk with wk):
 //   bra, H: the formulas of term_grad with Fw = Fb, ovw = ovb
 //   bra, S: d(ov)/dA_k = ov (-Dk Dk^T - 1.5 Bi + 0.75 A_k^-1), d(ov)/ds_k = -2 ov Y
-// and the ket formulas of term_sym with the same split (koH, koS).
+// and the ket formulas of term_sym with the same split.  The ket values of H
+// and of S for field f go out together: ko.put(f, vH, vS) / ko.add(f, vH, vS).
 // mid(i) is called at two points of the body (i = 1 after B, Bi, T and ov;
 // i = 2 after tau and sig), for callers that synchronise warps there.
 struct NoMid {
@@ -789,7 +793,7 @@ struct NoMid {
 #pragma nv_exec_check_disable
 template <int N, typename R, typename BA, typename KA, typename ACC, typename KOUT, typename MID = NoMid>
 NECG_HD bool term_fused(const BA &b, const KA &kr, const Consts<N> &cs, R wb, R wk, ACC &accH, ACC &accS,
-                        KOUT &koH, KOUT &koS, R &h_out, R &ov_out, const MID &mid = MID{}) {
+                        KOUT &ko, R &h_out, R &ov_out, const MID &mid = MID{}) {
     using KL = KetLayout<N>;
     using BL = BraLayout<N>;
     R Bi[tri(N)], T[3 * N], ov;
@@ -807,8 +811,7 @@ NECG_HD bool term_fused(const BA &b, const KA &kr, const Consts<N> &cs, R wb, R 
     const R Fk = wk * h, ovk = wk * ov;
     accH.d() += 0.75 * Fb;
     accS.d() += 0.75 * ovb;
-    koH.put(tri(N), 0.75 * Fk);
-    koS.put(tri(N), 0.75 * ovk);
+    ko.put(tri(N), 0.75 * Fk, 0.75 * ovk);
     // Bi (ovb (6 N_l' + W) - 1.5 Fb B) Bi = Bi ovb (6 N_l' + W) Bi - 1.5 Fb Bi, since
     // Bi B Bi = Bi (and the same for the ket)
     {
@@ -820,13 +823,11 @@ NECG_HD bool term_fused(const BA &b, const KA &kr, const Consts<N> &cs, R wb, R 
                            [&](int t, R v) { accH.g(t) = v; });
 #pragma unroll
         for (int t = 0; t < tri(N); ++t) W[t] = ovk * (6.0 * b(BL::Nk + t) + W[t]);
-        sandwich_seeded<N>(Bi, W, [&](int t) { return -(fk * Bi[t]); }, [&](int t, R v) { koH.put(t, v); });
         // S parts: Bi (-1.5 ov B) Bi = -1.5 ov Bi
+        sandwich_seeded<N>(Bi, W, [&](int t) { return -(fk * Bi[t]); },
+                           [&](int t, R v) { ko.put(t, v, -(sk * Bi[t])); });
 #pragma unroll
-        for (int t = 0; t < tri(N); ++t) {
-            accS.g(t) = accS.g(t) - sb * Bi[t];
-            koS.put(t, -(sk * Bi[t]));
-        }
+        for (int t = 0; t < tri(N); ++t) accS.g(t) = accS.g(t) - sb * Bi[t];
     }
     // Y = A_l' (T - S_l'); Qk = Bi (Z' - 4 A_l' M Y); Ql = Bi (Z' + 4 A_k M Y) = Qk + 4 M Y
     // (the difference of the two right-hand sides is 4 B M Y and Bi B = I)
@@ -837,22 +838,13 @@ NECG_HD bool term_fused(const BA &b, const KA &kr, const Consts<N> &cs, R wb, R 
     // the ket and bra matrices below are read once per element and used for
     // the three columns; each output's products are summed in the same order
 #pragma unroll
-    for (int i = 0; i < N; ++i) {
-        R s[3];
-        {
-            const R a = kr[KL::AMp + i * N];
+    for (int i = 0; i < N; ++i)
 #pragma unroll
-            for (int c = 0; c < 3; ++c) s[c] = a * Y[c];
+        for (int k = 0; k < N; ++k) {
+            const R a = kr[KL::AMn4 + i * N + k];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) Z[3 * i + c] += a * Y[3 * k + c];
         }
-#pragma unroll
-        for (int k = 1; k < N; ++k) {
-            const R a = kr[KL::AMp + i * N + k];
-#pragma unroll
-            for (int c = 0; c < 3; ++c) s[c] += a * Y[3 * k + c];
-        }
-#pragma unroll
-        for (int c = 0; c < 3; ++c) Z[3 * i + c] -= 4.0 * s[c];
-    }
     R Qk[3 * N], Ql[3 * N];
 #pragma unroll
     for (int i = 0; i < N; ++i)
@@ -867,10 +859,10 @@ NECG_HD bool term_fused(const BA &b, const KA &kr, const Consts<N> &cs, R wb, R 
     for (int i = 0; i < N; ++i)
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-            R s = cs.M[i * N] * Y[c];
+            R s = Qk[3 * i + c];
 #pragma unroll
-            for (int k = 1; k < N; ++k) s += cs.M[i * N + k] * Y[3 * k + c];
-            Ql[3 * i + c] = Qk[3 * i + c] + 4.0 * s;
+            for (int k = 0; k < N; ++k) s += cs.M4[i * N + k] * Y[3 * k + c];
+            Ql[3 * i + c] = s;
         }
     // H: bra s += 2 ovb A_k Qk - 2 Fb Y, ket 2 ovk A_l' Ql + 2 Fk Y ; S: -2 ovb Y, +2 ovk Y
     {
@@ -900,8 +892,7 @@ NECG_HD bool term_fused(const BA &b, const KA &kr, const Consts<N> &cs, R wb, R 
                 const R y = Y[3 * i + c];
                 accH.s(3 * i + c) = (accH.s(3 * i + c) - fb2 * y) + ob2 * s[c];
                 accS.s(3 * i + c) = accS.s(3 * i + c) - ob2 * y;
-                koH.put(tri(N) + 1 + 3 * i + c, ok2 * t[c] + fk2 * y);
-                koS.put(tri(N) + 1 + 3 * i + c, ok2 * y);
+                ko.put(tri(N) + 1 + 3 * i + c, ok2 * t[c] + fk2 * y, ok2 * y);
             }
         }
     }
@@ -937,8 +928,7 @@ NECG_HD bool term_fused(const BA &b, const KA &kr, const Consts<N> &cs, R wb, R 
             }
             accH.g(sx(i, j)) = s;
             accS.g(sx(i, j)) = accS.g(sx(i, j)) - ovb * dd;
-            koH.add(sx(i, j), -t);
-            koS.add(sx(i, j), -(ovk * ee));
+            ko.add(sx(i, j), -t, -(ovk * ee));
         }
     return ok;
 }

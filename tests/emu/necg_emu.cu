@@ -19,7 +19,10 @@ namespace {
 
 template <int N> Consts<N> consts(const double *mass, const double *ncv, double efs) {
     Consts<N> c;
-    for (int i = 0; i < N * N; ++i) c.M[i] = mass[i];
+    for (int i = 0; i < N * N; ++i) {
+        c.M[i] = mass[i];
+        c.M4[i] = 4.0 * mass[i];
+    }
     for (int q = 1; q <= N; ++q)
         for (int p = 0; p < q; ++p) c.cv[vidx(p, q)] = 2.0 * ncv[p] * ncv[q] / NECG_SQRT_PI;
     for (int i = 0; i < N; ++i) c.q[i] = ncv[i + 1];
@@ -169,6 +172,18 @@ struct RowOutH {
     double *r;
     void put(int f, CD v) { r[f] = v.v; }
     void add(int f, CD v) { r[f] += v.v; }
+};
+// the fused pass's ket output: the H and S values of one field together
+struct RowOutHS {
+    double *rh, *rs;
+    void put(int f, CD vh, CD vs) {
+        rh[f] = vh.v;
+        rs[f] = vs.v;
+    }
+    void add(int f, CD vh, CD vs) {
+        rh[f] += vh.v;
+        rs[f] += vs.v;
+    }
 };
 
 template <int N> int outprod_sym(const Args &a, const double *x, int LCe, int LCs, double *f, double *g, double *H,
@@ -325,11 +340,11 @@ template <int N> int outprod_fused(const Args &a, const double *x, int LCs, doub
                     for (int ff = 0; ff < PS; ++ff) rowsH[lane][ff] = rowsS[lane][ff] = 0.0;
                     if (k < K && l <= k) {
                         const double wk = l < k ? 2.0 * C[k] * krp[KetLayout<N>::winv] : 0.0;
-                        RowOutH roH{rowsH[lane]}, roS{rowsS[lane]};
+                        RowOutHS ro{rowsH[lane], rowsS[lane]};
                         CD h, ov;
                         if (!term_fused<N, CD>(HostBra{bra.data() + k, (size_t)K}, HostKet{krp}, cs,
-                                               CD(krp[KetLayout<N>::wC]), CD(wk), accH[lane], accS[lane], roH,
-                                               roS, h, ov))
+                                               CD(krp[KetLayout<N>::wC]), CD(wk), accH[lane], accS[lane], ro, h,
+                                               ov))
                             flags |= 1;
                         const double w = krp[KetLayout<N>::w];
                         hsum[lane] += w * h.v;
@@ -561,11 +576,11 @@ template <int N> int shard_pairs(const Args &a, const double *x, int LCs, int t0
                     for (int ff = 0; ff < PS; ++ff) rowsH[lane][ff] = rowsS[lane][ff] = 0.0;
                     if (k < K && l <= k) {
                         const double wk = l < k ? 2.0 * C[k] * krp[KetLayout<N>::winv] : 0.0;
-                        RowOutH roH{rowsH[lane]}, roS{rowsS[lane]};
+                        RowOutHS ro{rowsH[lane], rowsS[lane]};
                         CD h, ov;
                         if (!term_fused<N, CD>(HostBra{bra.data() + k, (size_t)K}, HostKet{krp}, cs,
-                                               CD(krp[KetLayout<N>::wC]), CD(wk), accH[lane], accS[lane], roH,
-                                               roS, h, ov))
+                                               CD(krp[KetLayout<N>::wC]), CD(wk), accH[lane], accS[lane], ro, h,
+                                               ov))
                             flags |= 1;
                         hsum[lane] += krp[KetLayout<N>::w] * h.v;
                         ssum[lane] += krp[KetLayout<N>::w] * ov.v;
