@@ -78,7 +78,9 @@ def parse():
     return ap.parse_args()
 
 
-DEFAULT_TILES = {"lc_e": 2, "minb_e": 16, "lc_g": 4, "minb_g": 8, "sym": 2, "lc_s": 2, "minw_s": 248}
+DEFAULT_TILES = {"lc_e": 2, "minb_e": 16, "lc_g": 4, "minb_g": 8, "sym": 2, "lc_s": 2, "minw_s": 268}
+# the fused-pass variant measured fastest for other n (n = 3: one-warp blocks, 12 per SM)
+DEFAULT_FUSED = {3: {"lc_s": 2, "minw_s": 122}}
 PASS_MODE = {"ordered": 0, "symmetric": 1, "fused": 2}
 # FP64 FLOPs per (k, l, P) term (FMA = 2; each div/sqrt/rsqrt/exp = 1), frozen at
 # the counts the kernels' own templates gave when the fused pass was first
@@ -288,7 +290,7 @@ def run_engine(args):
     x = torch.from_numpy(prob.x).cuda()
     from nbo_correlatedgaussians_b200.autotune import apply, tuned
     if args.no_tune:
-        tiles = dict(DEFAULT_TILES)
+        tiles = dict(DEFAULT_TILES, **DEFAULT_FUSED.get(prob.n, {}))
     else:
         tiles = dict(tuned(eng, x, prob.K))  # untimed; cached per (GPU, n, nst, K bucket)
     if args.pair_pass != "auto":

@@ -464,11 +464,12 @@ NECG_HD bool term_core(const BA &b, const KA &kr, const Consts<N> &cs, R (&Bi)[t
 // tau = 3 tr(M X) - 2 <Y, M Y>.  tr(M X) with X = A_k Bi A_l' is written through
 // the matrix with the smaller tr(M A): X = A_s - A_s Bi A_s, which keeps the
 // subtraction free of cancellation.  The choice differs from lane to lane, so
-// both N_s are read and one is selected (no divergent branch).
+// both N_s are read and one is selected (no divergent branch).  Y = A_l' (T - S_l')
+// is returned for the gradient formulas.
 #pragma nv_exec_check_disable
 template <int N, typename R, typename BA, typename KA>
 NECG_HD R term_tau(const BA &b, const KA &kr, const Consts<N> &cs, const R (&Bi)[tri(N)],
-                   const R (&T)[3 * N]) {
+                   const R (&T)[3 * N], R (&Y)[3 * N]) {
     using KL = KetLayout<N>;
     using BL = BraLayout<N>;
     R tMX;
@@ -488,7 +489,7 @@ NECG_HD R term_tau(const BA &b, const KA &kr, const Consts<N> &cs, const R (&Bi)
     }
     R yMy = R(0.0);
     {
-        R Dl[3 * N], Y[3 * N];
+        R Dl[3 * N];
 #pragma unroll
         for (int t = 0; t < 3 * N; ++t) Dl[t] = T[t] - kr[KL::Sp + t];
         symv3<N>(kr, KL::Ap, Dl, Y);
@@ -503,6 +504,13 @@ NECG_HD R term_tau(const BA &b, const KA &kr, const Consts<N> &cs, const R (&Bi)
             }
     }
     return 3.0 * tMX - 2.0 * yMy;
+}
+#pragma nv_exec_check_disable
+template <int N, typename R, typename BA, typename KA>
+NECG_HD R term_tau(const BA &b, const KA &kr, const Consts<N> &cs, const R (&Bi)[tri(N)],
+                   const R (&T)[3 * N]) {
+    R Y[3 * N];
+    return term_tau<N>(b, kr, cs, Bi, T, Y);
 }
 
 #pragma nv_exec_check_disable
@@ -786,7 +794,12 @@ NECG_HD bool term_sym(const BA &b, const KA &kr, const Consts<N> &cs, R E, R wb,
 // and the ket formulas of term_sym with the same split.  The ket values of H
 // and of S for field f go out together: ko.put(f, vH, vS) / ko.add(f, vH, vS).
 // mid(i) is called at two points of the body (i = 1 after B, Bi, T and ov;
-// i = 2 after tau and sig), for callers that synchronise warps there.
+// i = 2 after tau and sig), for callers that synchronise warps there.  tau's
+// Y = A_l' (T - S_l') goes on to the gradient formulas (it is not formed
+// twice).  For n <= 3 the Coulomb sum comes before tau (and before mid(2)),
+// otherwise after: the order that measured faster on a B200 for each n, since
+// the values live across the Coulomb sum (Y, or Z and W) set the register
+// pressure; the results are the same either way, bit for bit.
 struct NoMid {
     NECG_HD void operator()(int) const {}
 };
@@ -799,11 +812,13 @@ NECG_HD bool term_fused(const BA &b, const KA &kr, const Consts<N> &cs, R wb, R 
     R Bi[tri(N)], T[3 * N], ov;
     const bool ok = term_core<N>(b, kr, cs, Bi, T, ov);
     mid(1);
-    const R tau = term_tau<N>(b, kr, cs, Bi, T);
+    constexpr bool coulomb_first = N <= 3;
+    R Z[3 * N], W[tri(N)], rho, Y[3 * N];
+    if constexpr (coulomb_first) coulomb_grad<N>(Bi, T, cs, rho, Z, W);
+    const R tau = term_tau<N>(b, kr, cs, Bi, T, Y);
     const R sig = term_sig<N>(cs, T);
     mid(2);
-    R Z[3 * N], W[tri(N)], rho;
-    coulomb_grad<N>(Bi, T, cs, rho, Z, W);
+    if constexpr (!coulomb_first) coulomb_grad<N>(Bi, T, cs, rho, Z, W);
     const R h = ov * (2.0 * tau + rho - sig);
     h_out = h;
     ov_out = ov;
@@ -829,12 +844,11 @@ NECG_HD bool term_fused(const BA &b, const KA &kr, const Consts<N> &cs, R wb, R 
 #pragma unroll
         for (int t = 0; t < tri(N); ++t) accS.g(t) = accS.g(t) - sb * Bi[t];
     }
-    // Y = A_l' (T - S_l'); Qk = Bi (Z' - 4 A_l' M Y); Ql = Bi (Z' + 4 A_k M Y) = Qk + 4 M Y
-    // (the difference of the two right-hand sides is 4 B M Y and Bi B = I)
-    R Dl[3 * N], Y[3 * N];
+    // Qk = Bi (Z' - 4 A_l' M Y); Ql = Bi (Z' + 4 A_k M Y) = Qk + 4 M Y (the
+    // difference of the two right-hand sides is 4 B M Y and Bi B = I)
+    R Dl[3 * N];
 #pragma unroll
     for (int t = 0; t < 3 * N; ++t) Dl[t] = T[t] - kr[KL::Sp + t];
-    symv3<N>(kr, KL::Ap, Dl, Y);
     // the ket and bra matrices below are read once per element and used for
     // the three columns; each output's products are summed in the same order
 #pragma unroll
