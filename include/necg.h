@@ -94,7 +94,8 @@ int necg_set_variant(necg_handle *h, int minw_energy, int minw_grad);
  * copied while the current term runs), 248 (as 228 without the barrier after
  * every term), 258 and 268 (as 228, with warps 4-7 taking their per-term
  * barrier inside the term -- after the pair's Cholesky factor, inverse and
- * overlap for 258, after the kinetic and field terms for 268 -- so the two
+ * overlap for 258, after the kinetic and field terms (and, for n <= 3, the
+ * Coulomb sum) for 268 -- so the two
  * warps of each scheduler run different parts of the term), 222 and 232 (218
  * and 228 with 12 warps per block; NECG_ERR_UNSUPPORTED where their shared
  * memory does not fit, n = 5).  Set by the autotuner. */

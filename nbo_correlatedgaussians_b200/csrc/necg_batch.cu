@@ -33,7 +33,7 @@
 namespace necg {
 
 constexpr int kMaxN = 5;  // batched path: n <= 5 (He, H2, LiH and the like)
-constexpr int kConstsDoubles = 104;  // >= sizeof(Consts<6>) / 8
+constexpr int kConstsDoubles = 128;  // >= sizeof(Consts<6>) / 8
 
 struct InstDesc {
     int n, K, nst, lc_e, lc_g, nlc;
@@ -426,10 +426,8 @@ __global__ void __launch_bounds__(128) batch_reduce_kernel(PlanPtrs p) {
 template <int N> void fill_consts(InstDesc &d, const necg_handle *h) {
     static_assert(sizeof(Consts<N>) <= sizeof(d.cs), "constants do not fit");
     Consts<N> c;
-    for (int i = 0; i < N * N; ++i) {
-        c.M[i] = h->mass[i];
-        c.M4[i] = 4.0 * h->mass[i];
-    }
+    for (int i = 0; i < N * N; ++i) c.M[i] = h->mass[i];
+    c.derive();
     for (int q = 1; q <= N; ++q)
         for (int pp = 0; pp < q; ++pp)
             c.cv[vidx(pp, q)] = 2.0 * h->ncv[pp] * h->ncv[q] / NECG_SQRT_PI;

@@ -81,10 +81,8 @@ template <int N> void count_term(int which, long long &flops, long long &special
     std::vector<double> bra, ket;
     host_records<N>(bra, ket);
     Consts<N> cs;
-    for (int i = 0; i < N * N; ++i) {
-        cs.M[i] = (i % (N + 1) == 0) ? 0.5 : 0.01;
-        cs.M4[i] = 4.0 * cs.M[i];
-    }
+    for (int i = 0; i < N * N; ++i) cs.M[i] = (i % (N + 1) == 0) ? 0.5 : 0.01;
+    cs.derive();
     for (int t = 0; t < tri(N); ++t) cs.cv[t] = 1.0;
     for (int i = 0; i < N; ++i) cs.q[i] = -1.0;
     cs.efs = 1e-4;

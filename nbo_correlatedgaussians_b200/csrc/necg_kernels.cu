@@ -753,10 +753,8 @@ __global__ void reset_status_kernel(int *status) {
 // Host-side launchers (one instantiation per supported particle count)
 template <int N> Consts<N> make_consts(const double *mass, const double *ncv, double efs) {
     Consts<N> c;
-    for (int i = 0; i < N * N; ++i) {
-        c.M[i] = mass[i];
-        c.M4[i] = 4.0 * mass[i];
-    }
+    for (int i = 0; i < N * N; ++i) c.M[i] = mass[i];
+    c.derive();
     for (int q = 1; q <= N; ++q)
         for (int p = 0; p < q; ++p) c.cv[vidx(p, q)] = 2.0 * ncv[p] * ncv[q] / NECG_SQRT_PI;
     for (int i = 0; i < N; ++i) c.q[i] = ncv[i + 1];

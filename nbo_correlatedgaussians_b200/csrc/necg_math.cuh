@@ -109,10 +109,17 @@ template <int N> struct BraLayout {
 template <int N> struct Consts {
     double M[N * N];    // inverse-mass tensor, row-major
     double M4[N * N];   // 4 M (Q_l = Q_k + 4 M Y as one FMA chain per output)
+    double Mq[tri(N)];  // packed lower: M_ii on the diagonal, M_ik + M_ki below (quadratic forms in M)
     double cv[tri(N)];  // c_v for the n(n+1)/2 Coulomb pairs (p<q, q-major order)
     double q[N];        // ncv[1..n]
     double efs;
     double sqrt8n;      // sqrt(8^n)
+    // M4 and Mq from M
+    NECG_HD void derive() {
+        for (int i = 0; i < N * N; ++i) M4[i] = 4.0 * M[i];
+        for (int i = 0; i < N; ++i)
+            for (int k = 0; k <= i; ++k) Mq[sx(i, k)] = i == k ? M[i * N + i] : M[i * N + k] + M[k * N + i];
+    }
 };
 
 // Doubles of one part's compact output for one tile of a split lockstep group
@@ -476,16 +483,20 @@ NECG_HD R term_tau(const BA &b, const KA &kr, const Consts<N> &cs, const R (&Bi)
     {
         const R tl = kr[KL::tMA], tk = b(BL::tMA);
         const bool use_l = tl <= tk;
-        R acc = R(0.0);
+        // tr(Bi N_s): the diagonal and the off-diagonal products summed apart
+        R dg = R(0.0), od = R(0.0);
 #pragma unroll
         for (int i = 0; i < N; ++i)
 #pragma unroll
             for (int j = 0; j <= i; ++j) {
                 const R nl = kr[KL::Np + sx(i, j)], nk = b(BL::Nk + sx(i, j));
                 const R v = Bi[sx(i, j)] * (use_l ? nl : nk);
-                acc += (i == j) ? v : 2.0 * v;
+                if (i == j)
+                    dg = (i == 0) ? v : dg + v;
+                else
+                    od = (i == 1) ? v : od + v;
             }
-        tMX = (use_l ? tl : tk) - acc;
+        tMX = (use_l ? tl : tk) - (dg + 2.0 * od);
     }
     R yMy = R(0.0);
     {
@@ -493,13 +504,14 @@ NECG_HD R term_tau(const BA &b, const KA &kr, const Consts<N> &cs, const R (&Bi)
 #pragma unroll
         for (int t = 0; t < 3 * N; ++t) Dl[t] = T[t] - kr[KL::Sp + t];
         symv3<N>(kr, KL::Ap, Dl, Y);
+        // <Y, M Y> = sum_c sum_i Y_ic (M_ii Y_ic + sum_{k<i} (M_ik + M_ki) Y_kc)
 #pragma unroll
         for (int i = 0; i < N; ++i)
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
-                R s = cs.M[i * N] * Y[c];
+                R s = cs.Mq[sx(i, i)] * Y[3 * i + c];
 #pragma unroll
-                for (int k = 1; k < N; ++k) s += cs.M[i * N + k] * Y[3 * k + c];
+                for (int k = 0; k < i; ++k) s += cs.Mq[sx(i, k)] * Y[3 * k + c];
                 yMy += Y[3 * i + c] * s;
             }
     }
