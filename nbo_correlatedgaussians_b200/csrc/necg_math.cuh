@@ -310,29 +310,28 @@ NECG_HD void boys(R a, R bb, R &fs, R &D, R &ia, R &z) {
     const R ra = rsq(a);
     ia = ra * ra;
     z = bb * ia;
-    if (z <= NECG_F0_SPLIT) {
-        const R num = ((((NECG_PC1 * z + NECG_PC2) * z + NECG_PC3) * z + NECG_PC4) * z +
-                       NECG_PC5) * z + 1.0;
-        const R den = (((((NECG_PC6 * z + NECG_PC7) * z + NECG_PC8) * z + NECG_PC9) * z +
-                        NECG_PC10) * z + NECG_PC11) * z + 1.0;
-        const R q = rsq(num * den);
-        const R F0 = num * q;
-        fs = F0 * ra;
-        if (GRAD) {
-            const R dNh = (((2.5 * NECG_PC1 * z + 2.0 * NECG_PC2) * z + 1.5 * NECG_PC3) * z +
-                           NECG_PC4) * z + 0.5 * NECG_PC5;
-            const R dDh = ((((3.0 * NECG_PC6 * z + 2.5 * NECG_PC7) * z + 2.0 * NECG_PC8) * z +
-                            1.5 * NECG_PC9) * z + NECG_PC10) * z + 0.5 * NECG_PC11;
-            D = (q * q) * (dNh * den - dDh * num);
-        } else {
-            D = R(0.0);
-        }
+    // the branch is taken per lane; both forms share one reciprocal square root
+    // (of num den, or of bb), and the Pade polynomials are evaluated on every
+    // lane, so that the lanes of a warp on either side of the split run the
+    // same instructions
+    const bool pade = z <= NECG_F0_SPLIT;
+    const R num = ((((NECG_PC1 * z + NECG_PC2) * z + NECG_PC3) * z + NECG_PC4) * z + NECG_PC5) * z + 1.0;
+    const R den = (((((NECG_PC6 * z + NECG_PC7) * z + NECG_PC8) * z + NECG_PC9) * z + NECG_PC10) * z +
+                   NECG_PC11) * z + 1.0;
+    const R q = rsq(pade ? num * den : bb);
+    // Pade: F0 = num q, fs = F0 ra; asymptotic: F0 = sqrt(pi / (4 z)), F0 a^-1/2 = sqrt(pi / (4 bb))
+    const R fp = (num * q) * ra, fa = (0.5 * NECG_SQRT_PI) * q;
+    fs = pade ? fp : fa;
+    if (GRAD) {
+        const R dNh = (((2.5 * NECG_PC1 * z + 2.0 * NECG_PC2) * z + 1.5 * NECG_PC3) * z + NECG_PC4) * z +
+                      0.5 * NECG_PC5;
+        const R dDh = ((((3.0 * NECG_PC6 * z + 2.5 * NECG_PC7) * z + 2.0 * NECG_PC8) * z + 1.5 * NECG_PC9) * z +
+                       NECG_PC10) * z + 0.5 * NECG_PC11;
+        const R qq = q * q;
+        const R dp = qq * (dNh * den - dDh * num), da = -0.5 * a * qq;  // F0' / F0 = -1 / (2 z)
+        D = pade ? dp : da;
     } else {
-        // F0 = sqrt(pi / (4 z)) ; F0 a^-1/2 = sqrt(pi / (4 bb))
-        const R rb = rsq(bb);
-        fs = (0.5 * NECG_SQRT_PI) * rb;
-        if (GRAD) D = -0.5 * a * (rb * rb);  // F0' / F0 = -1 / (2 z)
-        else D = R(0.0);
+        D = R(0.0);
     }
 }
 

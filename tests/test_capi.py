@@ -67,8 +67,9 @@ def test_term_flops_counter(L):
     # the current count of an ordered n = 5 gradient term (3337 before the
     # Coulomb derivative coefficients shared one product per pair, 3307 before
     # the factor -4 of Z's update moved into the ket record, 3292 before tau's
-    # trace and quadratic form used the symmetric packed forms)
-    assert L.necg_term_flops(5, 1, None) == 3222
+    # trace and quadratic form used the symmetric packed forms, 3222 before the
+    # Boys function evaluated both of its branches' last products on every lane)
+    assert L.necg_term_flops(5, 1, None) == 3267
     for n in range(1, 7):
         e, g, y, f = (L.necg_term_flops(n, w, None) for w in range(4))
         # an unordered term carries both gradients, so it costs less than two
