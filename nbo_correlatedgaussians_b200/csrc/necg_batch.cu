@@ -198,9 +198,10 @@ __global__ void __launch_bounds__(32, 8) batch_fused_warp_kernel(PlanPtrs p) {
 // queue of tile groups that runs over the instances in plan order (largest
 // tiles first) and over each instance's groups (one 32-row block, 8 consecutive
 // ket chunks, one per warp).  The warps of a block work on the same instance and
-// bras and step through their terms together; the group's bras are staged in
-// shared memory once, each warp's ket records too, in two buffers (fsym_tile
-// with BSYNC, SBRA, SKET).  Shared memory is sized for n = kMaxN.
+// bras; the group's bras are staged in shared memory once, each warp's ket
+// records too, in two buffers (fsym_tile with BSYNC, SBRA, SKET), and the warps
+// meet only at the group's barriers (no barrier per term, as the single-
+// instance variant 248).  Shared memory is sized for n = kMaxN.
 template <int N> __host__ __device__ constexpr int bfused_warp_smem() {
     return 2 * Part<N>::size * 32 + 2 * 16 * 33 + 64 + 2 * KetLayout<N>::size;
 }
@@ -225,9 +226,9 @@ __device__ __forceinline__ void batch_fused_group(const InstDesc &d, int2 gr, do
     }
     __syncthreads();
     double *part_b = d.psym, *part_k = d.psym + (size_t)d.nstiles * 2 * PS * 32;
-    fsym_tile<N, true, true, true, true>(d.stile_start[kb] + lc, make_int2(kb, lc), d.lc_s, K, d.nst,
-                                         consts_of<N>(d), d.bra, d.ket, d.C, d.kmap, d.H, d.S, part_b, part_k,
-                                         d.status, sm, idle, sbra);
+    fsym_tile<N, true, true, true, true, 3>(d.stile_start[kb] + lc, make_int2(kb, lc), d.lc_s, K, d.nst,
+                                            consts_of<N>(d), d.bra, d.ket, d.C, d.kmap, d.H, d.S, part_b, part_k,
+                                            d.status, sm, idle, sbra);
     __syncthreads();  // sbra and the warps' areas are reused by the next group
 }
 
