@@ -41,6 +41,7 @@ inline bool operator<=(CD a, CD b) { return a.v <= b.v; }
 inline CD sqrt(CD a) { ++count_ctx().special; return CD(::sqrt(a.v)); }
 inline CD rsqrt(CD a) { ++count_ctx().special; return CD(1.0 / ::sqrt(a.v)); }
 inline CD rsq(CD a) { return rsqrt(a); }
+inline CD rcp(CD a) { return CD(1.0) / a; }
 inline CD exp(CD a) { ++count_ctx().special; return CD(::exp(a.v)); }
 inline double val(CD x) { return x.v; }
 

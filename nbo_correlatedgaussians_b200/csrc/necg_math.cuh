@@ -215,6 +215,22 @@ NECG_HD double rsq(double x) {
 #endif
 }
 
+// 1/x for normal, positive x.  On the device the hardware approximation
+// rcp.approx.ftz.f64 is refined by one third-order step: with e = 1 - x y,
+// y <- y + y (e + e^2), the series of 1 / (1 - e) to second order, whose
+// truncation error (of order e^3) lies far below the result's rounding.  Host
+// builds (the emulator) use 1 / x.
+NECG_HD double rcp(double x) {
+#ifdef __CUDA_ARCH__
+    double y;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+    const double e = fma(-x, y, 1.0);
+    return fma(y, fma(e, e, e), y);
+#else
+    return 1.0 / x;
+#endif
+}
+
 // Cholesky of a packed SPD matrix B = R R^T; returns the inverse Bi (packed),
 // prod(1/R_ii) and a success flag.  Fully unrolled into registers.
 #pragma nv_exec_check_disable
@@ -295,40 +311,68 @@ NECG_HD void symv3(const Acc &S, int off, const R (&x)[3 * N], R (&y)[3 * N]) {
 
 // Boys-function pieces for one Coulomb pair.  Given a = v^T Bi v and
 // bb = |v^T T|^2 (z = bb / a) returns fs = F0(z) a^{-1/2} and, when GRAD,
-// D = F0'(z) / F0(z) (so F0'(z) a^{-1/2} = fs D) and ia = 1/a.  The Pade branch (z <= 16.3578) and the
-// asymptotic branch sqrt(pi/(4z)) follow python/utils.py:78-106; in the Pade
-// branch F0 = sqrt(num / den).  Two reciprocal square roots give every
-// quotient and root needed:
-//   ra = a^{-1/2}:          1/a = ra^2,  fs = F0 ra
-//   q = (num den)^{-1/2}:   F0 = num q,  q^2 = 1 / (num den)
-// and, from F0^2 = num / den, F0' = F0 (num'/num - den'/den) / 2, so
-//   D = F0' / F0 = q^2 (num' den - den' num) / 2,
-// with num'/2 and den'/2 evaluated directly (halved coefficients: exact).
+// D = F0'(z) / F0(z) (so F0'(z) a^{-1/2} = fs D) and ia = 1/a.  The Pade branch
+// (z <= 16.3578) and the asymptotic branch sqrt(pi/(4z)) follow
+// python/utils.py:78-106; in the Pade branch F0 = sqrt(num / den), and from
+// F0^2 = num / den, F0' = F0 (num'/num - den'/den) / 2, so
+//   D = F0' / F0 = (num' den - den' num) / (2 num den)  (Pade),  -1 / (2 z)  (asymptotic),
+// with num'/2 and den'/2 evaluated directly (halved coefficients: exact).  Two
+// special functions give every quotient and root; RCP chooses between two ways:
+//   RCP:   ia = 1/a (rcp);  q = (num den a)^{-1/2} (Pade) or bb^{-1/2}:
+//          fs = num q or (sqrt(pi) / 2) q, and q^2 a = 1 / (num den) or 1 / z;
+//   !RCP:  ra = a^{-1/2}, ia = ra^2;  q = (num den)^{-1/2} or bb^{-1/2}:
+//          fs = num q ra or (sqrt(pi) / 2) q, and q^2 = 1 / (num den) or 1 / bb.
+// RCP takes four FP64 operations fewer per pair but holds more values at once;
+// it is used where it timed faster on a B200 (n > 3).  The branch is taken per
+// lane: every lane evaluates the Pade polynomials and the two forms differ only
+// in the operand of the square root and in the factors selected, so that the
+// lanes of a warp on either side of the split run the same instructions.
+template <typename R> NECG_HD void boys_pade(R z, R &num, R &den) {
+    num = ((((NECG_PC1 * z + NECG_PC2) * z + NECG_PC3) * z + NECG_PC4) * z + NECG_PC5) * z + 1.0;
+    den = (((((NECG_PC6 * z + NECG_PC7) * z + NECG_PC8) * z + NECG_PC9) * z + NECG_PC10) * z + NECG_PC11) * z + 1.0;
+}
+template <typename R> NECG_HD void boys_pade_dh(R z, R &dNh, R &dDh) {
+    dNh = (((2.5 * NECG_PC1 * z + 2.0 * NECG_PC2) * z + 1.5 * NECG_PC3) * z + NECG_PC4) * z + 0.5 * NECG_PC5;
+    dDh = ((((3.0 * NECG_PC6 * z + 2.5 * NECG_PC7) * z + 2.0 * NECG_PC8) * z + 1.5 * NECG_PC9) * z + NECG_PC10) * z +
+          0.5 * NECG_PC11;
+}
 #pragma nv_exec_check_disable
-template <bool GRAD, typename R>
+template <bool GRAD, bool RCP = true, typename R>
 NECG_HD void boys(R a, R bb, R &fs, R &D, R &ia, R &z) {
-    const R ra = rsq(a);
-    ia = ra * ra;
+    R ra = R(1.0);
+    if constexpr (RCP) {
+        ia = rcp(a);
+    } else {
+        ra = rsq(a);
+        ia = ra * ra;
+    }
     z = bb * ia;
-    // the branch is taken per lane; both forms share one reciprocal square root
-    // (of num den, or of bb), and the Pade polynomials are evaluated on every
-    // lane, so that the lanes of a warp on either side of the split run the
-    // same instructions
     const bool pade = z <= NECG_F0_SPLIT;
-    const R num = ((((NECG_PC1 * z + NECG_PC2) * z + NECG_PC3) * z + NECG_PC4) * z + NECG_PC5) * z + 1.0;
-    const R den = (((((NECG_PC6 * z + NECG_PC7) * z + NECG_PC8) * z + NECG_PC9) * z + NECG_PC10) * z +
-                   NECG_PC11) * z + 1.0;
-    const R q = rsq(pade ? num * den : bb);
-    // Pade: F0 = num q, fs = F0 ra; asymptotic: F0 = sqrt(pi / (4 z)), F0 a^-1/2 = sqrt(pi / (4 bb))
-    const R fp = (num * q) * ra, fa = (0.5 * NECG_SQRT_PI) * q;
-    fs = pade ? fp : fa;
+    R num, den;
+    boys_pade(z, num, den);
+    const R c = R(0.5 * NECG_SQRT_PI);
+    R q;
+    if constexpr (RCP) {
+        q = rsq(pade ? (num * den) * a : bb);
+        fs = (pade ? num : c) * q;
+    } else {
+        q = rsq(pade ? num * den : bb);
+        const R fp = (num * q) * ra, fa = c * q;
+        fs = pade ? fp : fa;
+    }
     if (GRAD) {
-        const R dNh = (((2.5 * NECG_PC1 * z + 2.0 * NECG_PC2) * z + 1.5 * NECG_PC3) * z + NECG_PC4) * z +
-                      0.5 * NECG_PC5;
-        const R dDh = ((((3.0 * NECG_PC6 * z + 2.5 * NECG_PC7) * z + 2.0 * NECG_PC8) * z + 1.5 * NECG_PC9) * z +
-                       NECG_PC10) * z + 0.5 * NECG_PC11;
-        const R qq = q * q;
-        const R dp = qq * (dNh * den - dDh * num), da = -0.5 * a * qq;  // F0' / F0 = -1 / (2 z)
+        R dNh, dDh;
+        boys_pade_dh(z, dNh, dDh);
+        R dp, da;
+        if constexpr (RCP) {
+            const R qa = (q * q) * a;
+            dp = qa * (dNh * den - dDh * num);
+            da = -0.5 * qa;
+        } else {
+            const R qq = q * q;
+            dp = qq * (dNh * den - dDh * num);
+            da = -0.5 * a * qq;
+        }
         D = pade ? dp : da;
     } else {
         D = R(0.0);
@@ -362,7 +406,7 @@ NECG_HD void coulomb_grad(const R (&Bi)[tri(N)], const R (&T)[3 * N], const Cons
             }
             const R bb = bv[0] * bv[0] + bv[1] * bv[1] + bv[2] * bv[2];
             R fs, D, ia, z;
-            boys<true>(a, bb, fs, D, ia, z);
+            boys<true, (N > 3)>(a, bb, fs, D, ia, z);
             // alpha = c F0' a^{-3/2} = c fs D / a, beta = c a^{-3/2} (z F0' + F0 / 2) = (c fs / a)(z D + 1/2)
             const R cf = cs.cv[vidx(p, q)] * fs;
             rho += cf;
@@ -559,7 +603,7 @@ NECG_HD bool term_energy(const BA &b, const KA &kr, const Consts<N> &cs, R &ov, 
             }
             const R bb = bv[0] * bv[0] + bv[1] * bv[1] + bv[2] * bv[2];
             R fs, D, ia, z;
-            boys<false>(a, bb, fs, D, ia, z);
+            boys<false, (N > 3)>(a, bb, fs, D, ia, z);
             r += cs.cv[vidx(p, q)] * fs;
         }
     rho = r;

@@ -68,8 +68,9 @@ def test_term_flops_counter(L):
     # Coulomb derivative coefficients shared one product per pair, 3307 before
     # the factor -4 of Z's update moved into the ket record, 3292 before tau's
     # trace and quadratic form used the symmetric packed forms, 3222 before the
-    # Boys function evaluated both of its branches' last products on every lane)
-    assert L.necg_term_flops(5, 1, None) == 3267
+    # Boys function evaluated both of its branches' last products on every lane,
+    # 3267 before it took 1/a from a reciprocal for n > 3)
+    assert L.necg_term_flops(5, 1, None) == 3237
     for n in range(1, 7):
         e, g, y, f = (L.necg_term_flops(n, w, None) for w in range(4))
         # an unordered term carries both gradients, so it costs less than two
