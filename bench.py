@@ -78,7 +78,7 @@ def parse():
     return ap.parse_args()
 
 
-DEFAULT_TILES = {"lc_e": 2, "minb_e": 16, "lc_g": 4, "minb_g": 8, "sym": 2, "lc_s": 2, "minw_s": 248}
+DEFAULT_TILES = {"lc_e": 2, "minb_e": 16, "lc_g": 4, "minb_g": 8, "sym": 2, "lc_s": 2, "minw_s": 268}
 # the fused-pass variant measured fastest for other n (n = 3: one-warp blocks, 12 per SM)
 DEFAULT_FUSED = {3: {"lc_s": 2, "minw_s": 122}}
 PASS_MODE = {"ordered": 0, "symmetric": 1, "fused": 2}

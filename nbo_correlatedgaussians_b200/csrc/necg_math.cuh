@@ -309,6 +309,21 @@ NECG_HD void symv3(const Acc &S, int off, const R (&x)[3 * N], R (&y)[3 * N]) {
     }
 }
 
+// y += S x for S symmetric (packed, read through an accessor) and x n x 3: the
+// products fuse into y's values
+#pragma nv_exec_check_disable
+template <int N, typename R, typename Acc>
+NECG_HD void symv3_acc(const Acc &S, int off, const R (&x)[3 * N], R (&y)[3 * N]) {
+#pragma unroll
+    for (int i = 0; i < N; ++i)
+#pragma unroll
+        for (int k = 0; k < N; ++k) {
+            const R a = S[off + sx(i, k)];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) y[3 * i + c] += a * x[3 * k + c];
+        }
+}
+
 // Boys-function pieces for one Coulomb pair.  Given a = v^T Bi v and
 // bb = |v^T T|^2 (z = bb / a) returns fs = F0(z) a^{-1/2} and, when GRAD,
 // D = F0'(z) / F0(z) (so F0'(z) a^{-1/2} = fs D) and ia = 1/a.  The Pade branch
@@ -316,7 +331,7 @@ NECG_HD void symv3(const Acc &S, int off, const R (&x)[3 * N], R (&y)[3 * N]) {
 // python/utils.py:78-106; in the Pade branch F0 = sqrt(num / den), and from
 // F0^2 = num / den, F0' = F0 (num'/num - den'/den) / 2, so
 //   D = F0' / F0 = (num' den - den' num) / (2 num den)  (Pade),  -1 / (2 z)  (asymptotic),
-// with num'/2 and den'/2 evaluated directly (halved coefficients: exact).  Two
+// with num'/2 den - den'/2 num evaluated as one polynomial.  Two
 // special functions give every quotient and root; RCP chooses between two ways:
 //   RCP:   ia = 1/a (rcp);  q = (num den a)^{-1/2} (Pade) or bb^{-1/2}:
 //          fs = num q or (sqrt(pi) / 2) q, and q^2 a = 1 / (num den) or 1 / z;
@@ -331,10 +346,29 @@ template <typename R> NECG_HD void boys_pade(R z, R &num, R &den) {
     num = ((((NECG_PC1 * z + NECG_PC2) * z + NECG_PC3) * z + NECG_PC4) * z + NECG_PC5) * z + 1.0;
     den = (((((NECG_PC6 * z + NECG_PC7) * z + NECG_PC8) * z + NECG_PC9) * z + NECG_PC10) * z + NECG_PC11) * z + 1.0;
 }
-template <typename R> NECG_HD void boys_pade_dh(R z, R &dNh, R &dDh) {
-    dNh = (((2.5 * NECG_PC1 * z + 2.0 * NECG_PC2) * z + 1.5 * NECG_PC3) * z + NECG_PC4) * z + 0.5 * NECG_PC5;
-    dDh = ((((3.0 * NECG_PC6 * z + 2.5 * NECG_PC7) * z + 2.0 * NECG_PC8) * z + 1.5 * NECG_PC9) * z + NECG_PC10) * z +
-          0.5 * NECG_PC11;
+// (num' den - den' num) / 2 as one polynomial of degree 10: its coefficients
+// are those of num'/2 den - den'/2 num, formed from the Pade coefficients when
+// the code is compiled
+struct BoysDP {
+    double c[11];
+    constexpr BoysDP() : c{} {
+        const double nh[5] = {0.5 * NECG_PC5, NECG_PC4, 1.5 * NECG_PC3, 2.0 * NECG_PC2, 2.5 * NECG_PC1};  // num'/2
+        const double de[7] = {1.0, NECG_PC11, NECG_PC10, NECG_PC9, NECG_PC8, NECG_PC7, NECG_PC6};       // den
+        const double dh[6] = {0.5 * NECG_PC11, NECG_PC10, 1.5 * NECG_PC9, 2.0 * NECG_PC8, 2.5 * NECG_PC7,
+                              3.0 * NECG_PC6};                                                         // den'/2
+        const double nu[6] = {1.0, NECG_PC5, NECG_PC4, NECG_PC3, NECG_PC2, NECG_PC1};                  // num
+        for (int i = 0; i < 5; ++i)
+            for (int j = 0; j < 7; ++j) c[i + j] += nh[i] * de[j];
+        for (int i = 0; i < 6; ++i)
+            for (int j = 0; j < 6; ++j) c[i + j] -= dh[i] * nu[j];
+    }
+};
+template <typename R> NECG_HD R boys_pade_dp(R z) {
+    constexpr BoysDP p{};
+    R v = R(p.c[10]) * z + p.c[9];
+#pragma unroll
+    for (int k = 8; k >= 0; --k) v = v * z + p.c[k];
+    return v;
 }
 #pragma nv_exec_check_disable
 template <bool GRAD, bool RCP = true, typename R>
@@ -361,16 +395,15 @@ NECG_HD void boys(R a, R bb, R &fs, R &D, R &ia, R &z) {
         fs = pade ? fp : fa;
     }
     if (GRAD) {
-        R dNh, dDh;
-        boys_pade_dh(z, dNh, dDh);
+        const R P = boys_pade_dp(z);
         R dp, da;
         if constexpr (RCP) {
             const R qa = (q * q) * a;
-            dp = qa * (dNh * den - dDh * num);
+            dp = qa * P;
             da = -0.5 * qa;
         } else {
             const R qq = q * q;
-            dp = qq * (dNh * den - dDh * num);
+            dp = qq * P;
             da = -0.5 * a * qq;
         }
         D = pade ? dp : da;
@@ -543,10 +576,10 @@ NECG_HD R term_tau(const BA &b, const KA &kr, const Consts<N> &cs, const R (&Bi)
     }
     R yMy = R(0.0);
     {
-        R Dl[3 * N];
+        // Y = A_l' (T - S_l') = A_l' T - A_l' S_l', the second product from the ket record
 #pragma unroll
-        for (int t = 0; t < 3 * N; ++t) Dl[t] = T[t] - kr[KL::Sp + t];
-        symv3<N>(kr, KL::Ap, Dl, Y);
+        for (int t = 0; t < 3 * N; ++t) Y[t] = -kr[KL::ASp + t];
+        symv3_acc<N>(kr, KL::Ap, T, Y);
         // <Y, M Y> = sum_c sum_i Y_ic (M_ii Y_ic + sum_{k<i} (M_ik + M_ki) Y_kc)
 #pragma unroll
         for (int i = 0; i < N; ++i)

@@ -69,8 +69,9 @@ def test_term_flops_counter(L):
     # the factor -4 of Z's update moved into the ket record, 3292 before tau's
     # trace and quadratic form used the symmetric packed forms, 3222 before the
     # Boys function evaluated both of its branches' last products on every lane,
-    # 3267 before it took 1/a from a reciprocal for n > 3)
-    assert L.necg_term_flops(5, 1, None) == 3237
+    # 3267 before it took 1/a from a reciprocal for n > 3, 3237 before F0'/F0's
+    # numerator became one polynomial)
+    assert L.necg_term_flops(5, 1, None) == 3222
     for n in range(1, 7):
         e, g, y, f = (L.necg_term_flops(n, w, None) for w in range(4))
         # an unordered term carries both gradients, so it costs less than two
